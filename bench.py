@@ -1,0 +1,416 @@
+#!/usr/bin/env python3
+"""Benchmark of the beta(r,VS) SpMV hot path on B200 -- one JSON line.
+
+Workload (default): FP64 SpMV across all formats beta(1,8), beta(2,8),
+beta(4,8), beta(8,8) on the seeded power-law matrix (N = 4,000,000, row
+lengths min(2000, Zipf(1.8) + 3), 70% of each row in diagonal-centred runs,
+values U[-1,1], seed 1; ~63.4M nnz, int32 indices).  One step = one
+y += A x per format (4 SpMV launches), inputs resident in HBM.
+
+* ``value``   -- algorithmic GB/s of the whole step (bytes of values,
+  headers, block-row pointer, x once and y read+write, per SpMV), summed
+  over ranks, divided by the max-over-ranks device time.
+* ``e2e``     -- the same bytes per step over the time of the public call
+  sequence with HOST buffers: pinned x and y copied in, the 4 SpMVs, y
+  copied back, every step.
+* ``roofline``-- the SpMV kernel: algorithmic bytes per launch / mean
+  CUDA-event launch time, against the measured HBM copy bandwidth.
+* ``mixed``   -- the same matrix in the f32 beta(r,16) layout with FP32 x
+  and FP64 accumulation: GB/s, SpMV/s ratio to FP64 and max relative error
+  against the FP64 path (which is bit-identical to the reference).
+* ``cpu_baseline`` -- the reference's own AVX-512 OpenMP SpMV
+  (SPC5_Spmv_omp, src/spc5.hpp compiled by oracle/Makefile) on this host.
+
+``--impl reference`` runs only the reference CPU path with all host
+threads and prints its line.  Multi-GPU (torchrun): every rank runs its own
+copy of the workload (weak scaling); only barrier and max-reduction of the
+timings cross ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from spc5_b200 import matrices as M  # noqa: E402
+
+METRIC = "SpMV GB/s (algorithmic bytes, FP64, all beta(r,8) formats)"
+UNIT = "GB/s"
+FORMATS = (1, 2, 4, 8)
+
+
+def spmv_bytes(nnz, nblocks, r, nrows, ncols, value_bytes=8, mask_bytes=1, x_bytes=8, y_bytes=8):
+    """Algorithmic bytes of one y += A x in beta(r,VS):
+    nnz*sv + blocks*(4 + r*m) + 4*(ceil(N/r)+1) + ncols*sx + 2*N*sy."""
+    nbr = (nrows + r - 1) // r
+    return (nnz * value_bytes + nblocks * (4 + r * mask_bytes) + 4 * (nbr + 1) + ncols * x_bytes
+            + 2 * nrows * y_bytes)
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def build_workload(name):
+    if name == "powerlaw":
+        return M.powerlaw()
+    if name == "stencil27":
+        return M.stencil27(160)
+    if name == "poisson":
+        return M.poisson2d(512)
+    raise ValueError(name)
+
+
+def workload_desc(name, csr):
+    return {"powerlaw": "power-law N=4,000,000 Zipf(1.8)+3 clipped to 2000, 70% runs U[1,16] near "
+                        "diagonal (sigma N/100), U[-1,1] values, seed 1",
+            "stencil27": "27-point stencil 160^3, diag 26, neighbours -1+U[-1e-3,1e-3], seed 2",
+            "poisson": "5-point Poisson 512^2, diag 4, off -1"}[name] + f"; nnz={csr.nnz}"
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.out = None
+
+    def __enter__(self):
+        try:
+            self.out = open(os.devnull if False else f"/tmp/spc5_clocks_{os.getpid()}.csv", "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.out:
+            self.out.close()
+
+    def summary(self):
+        path = f"/tmp/spc5_clocks_{os.getpid()}.csv"
+        if not os.path.exists(path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        rows = []
+        with open(path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        load = [s for s in sm if mx and s > 0.3 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's OpenMP path
+# ---------------------------------------------------------------------------
+
+def cpu_baseline(csr, budget_s=20.0, formats=FORMATS):
+    """Times SPC5_{r}rVc_Spmv_omp of the compiled reference on this host.
+    Returns (GB/s, cores, description) over a bounded number of steps."""
+    import oracle
+    if not (oracle.ref_available() and oracle.cpu_has_avx512()):
+        return None
+    threads = oracle.ref().ref_max_threads()
+    xp = oracle.x_padded(M.x_vector(csr.ncols, 0))
+    mats, total_bytes = [], 0
+    for r in formats:
+        m = oracle.RefMatrix(csr.rowptr, csr.colidx, csr.values, csr.ncols)
+        nb = m.convert(r)
+        m.split(threads)
+        mats.append(m)
+        total_bytes += spmv_bytes(csr.nnz, nb, r, csr.nrows, csr.ncols)
+    y = np.zeros(csr.nrows + 8)
+    for m in mats:  # warm-up
+        m.time_spmv_omp(xp, y, 1)
+    t0 = time.perf_counter()
+    steps, secs = 0, 0.0
+    while secs < budget_s and steps < 64:
+        for m in mats:
+            secs += m.time_spmv_omp(xp, y, 1)
+        steps += 1
+        if time.perf_counter() - t0 > 2 * budget_s:
+            break
+    gbs = total_bytes * steps / secs / 1e9
+    return gbs, threads, steps, secs
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libspc5ref.so was not built"}))
+        return 0
+    if not oracle.cpu_has_avx512():
+        print(json.dumps({"impl": "reference", "unavailable": "host CPU has no AVX-512 (reference build "
+                                                               "uses USE_AVX512 kernels)"}))
+        return 0
+    csr = build_workload(args.workload)
+    threads = oracle.ref().ref_max_threads()
+    xp = oracle.x_padded(M.x_vector(csr.ncols, 0))
+    mats, step_bytes = [], 0
+    for r in FORMATS:
+        m = oracle.RefMatrix(csr.rowptr, csr.colidx, csr.values, csr.ncols)
+        nb = m.convert(r)
+        m.split(threads)
+        mats.append(m)
+        step_bytes += spmv_bytes(csr.nnz, nb, r, csr.nrows, csr.ncols)
+    y = np.zeros(csr.nrows + 8)
+    for _ in range(args.warmup):
+        for m in mats:
+            m.time_spmv_omp(xp, y, 1)
+    secs = 0.0
+    for _ in range(args.steps):
+        for m in mats:
+            secs += m.time_spmv_omp(xp, y, 1)
+    value = step_bytes * args.steps / secs / 1e9
+    line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(secs / args.steps * 1e3, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "desc": workload_desc(args.workload, csr),
+                       "formats": list(FORMATS), "l2": "inputs larger than L2"},
+            "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": f"{args.steps} steps x 4 SPC5_Spmv_omp calls (r=1,2,4,8) on the full "
+                                       f"matrix, OMP threads={threads}"},
+            "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU path
+# ---------------------------------------------------------------------------
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+
+    import spc5_b200 as S
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    csr = build_workload(args.workload)
+    stream = torch.cuda.current_stream()
+    mats, bytes_of = [], {}
+    for r in FORMATS:
+        m = S.csr_matrix(csr.rowptr, csr.colidx, csr.values, csr.ncols)
+        S.CSR_to_SPC5(m, S.FORMAT_OF_R[r])
+        mats.append((r, m))
+        bytes_of[r] = spmv_bytes(csr.nnz, m.numberOfBlocks, r, csr.nrows, csr.ncols)
+    step_bytes = sum(bytes_of.values())
+    x = torch.from_numpy(M.x_vector(csr.ncols, 0)).to(dev)
+    y = torch.zeros(csr.nrows, dtype=torch.float64, device=dev)
+
+    def step(events=None):
+        for i, (r, m) in enumerate(mats):
+            if events is not None:
+                events[i][0].record(stream)
+            S.SPC5_Spmv(m, x, y)
+            if events is not None:
+                events[i][1].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # ---- device-timed region (inputs resident, larger than L2) ----
+    launch_ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                  for _ in mats] for _ in range(args.steps)]
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        t_start.record(stream)
+        for k in range(args.steps):
+            step(launch_ev[k])
+        t_end.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    clocks = clk.summary()
+    ms_local = t_start.elapsed_time(t_end)
+    ms = max_over_ranks(ms_local)
+    value = step_bytes * args.steps * world / (ms * 1e-3) / 1e9
+    per_r_ms = {r: statistics.mean(launch_ev[k][i][0].elapsed_time(launch_ev[k][i][1]) for k in range(args.steps))
+                for i, (r, _) in enumerate(mats)}
+    kernel_ms = sum(per_r_ms.values())
+    achieved = step_bytes / (kernel_ms * 1e-3) / 1e9
+    peak, peak_kind = load_peaks()
+
+    # ---- e2e through the public API with host buffers ----
+    x_host = torch.from_numpy(M.x_vector(csr.ncols, 0)).pin_memory()
+    y_host = torch.zeros(csr.nrows, dtype=torch.float64).pin_memory()
+    xd = torch.empty_like(x)
+    yd = torch.empty_like(y)
+
+    def e2e_step():
+        xd.copy_(x_host, non_blocking=True)
+        yd.copy_(y_host, non_blocking=True)
+        for r, m in mats:
+            S.SPC5_Spmv(m, xd, yd)
+        y_host.copy_(yd, non_blocking=True)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e_value = step_bytes * args.steps * world / (e2e_ms * 1e-3) / 1e9
+
+    # ---- mixed precision on the same matrix (f32 beta(r,16), FP64 y) ----
+    mixed = {}
+    if not args.no_mixed:
+        y_ref = torch.zeros_like(y)
+        x32 = x.float()
+        mixed_ms_total, fp64_ms_total, mixed_bytes, max_rel = 0.0, 0.0, 0, 0.0
+        for r, m64 in mats:
+            m32 = S.csr_matrix(csr.rowptr, csr.colidx, csr.values, csr.ncols, dtype=np.float32)
+            S.CSR_to_SPC5(m32, S.FORMAT_OF_R[r])
+            ym = torch.zeros_like(y)
+            y_ref.zero_()
+            S.SPC5_Spmv(m64, x, y_ref)
+            S.SPC5_Spmv_mixed(m32, x32, ym)
+            torch.cuda.synchronize()
+            rel = ((ym - y_ref).abs().max() / y_ref.abs().max()).item()
+            max_rel = max(max_rel, rel)
+            for _ in range(args.warmup):
+                S.SPC5_Spmv_mixed(m32, x32, ym)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(args.steps):
+                S.SPC5_Spmv_mixed(m32, x32, ym)
+            b.record(stream)
+            torch.cuda.synchronize()
+            mixed_ms_total += a.elapsed_time(b) / args.steps
+            fp64_ms_total += per_r_ms[r]
+            mixed_bytes += spmv_bytes(csr.nnz, m32.numberOfBlocks, r, csr.nrows, csr.ncols, 4, 2, 4, 8)
+            del m32
+        mixed = {"gbs": round(mixed_bytes / (mixed_ms_total * 1e-3) / 1e9, 2),
+                 "spmv_per_s_ratio_vs_fp64": round(fp64_ms_total / mixed_ms_total, 3),
+                 "normwise_rel_err_vs_fp64": max_rel, "layout": "f32 beta(r,16), FP32 x, FP64 y"}
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline:
+            res = cpu_baseline(csr)
+            if res is not None:
+                gbs, threads, nsteps, secs = res
+                cpu = {"value": round(gbs, 3), "unit": UNIT, "cores": threads, "kind": "reference",
+                       "sample": f"{nsteps} steps x 4 SPC5_Spmv_omp (r=1,2,4,8) on the full matrix, "
+                                 f"{secs:.1f} s"}
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "desc": workload_desc(args.workload, csr),
+                       "formats": list(FORMATS), "nrows": csr.nrows, "nnz": csr.nnz,
+                       "blocks": {str(r): m.numberOfBlocks for r, m in mats},
+                       "l2": "inputs larger than L2 (4 matrices of >0.5 GB read in turn)",
+                       "parallelism": f"replica per GPU x{world}"},
+            "per_format_gbs": {str(r): round(bytes_of[r] / (per_r_ms[r] * 1e-3) / 1e9, 2) for r in FORMATS},
+            "gflops": round(2 * csr.nnz * len(FORMATS) * args.steps * world / (ms * 1e-3) / 1e9, 2),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                         "traffic": args.traffic, "kernel": "k_spmv_groups (all r)"},
+            "e2e": {"value": round(e2e_value, 2), "unit": UNIT,
+                    "h2d_bytes_per_step": int(x.numel() * 8 + y.numel() * 8),
+                    "d2h_bytes_per_step": int(y.numel() * 8)},
+            "gpu_launches": len(FORMATS) * args.steps,
+            "clocks": clocks,
+            "mixed": mixed,
+            "cpu_baseline": cpu,
+        }
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["powerlaw", "stencil27", "poisson"], default="powerlaw")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--traffic", type=float, default=None,
+                    help="ncu dram bytes per launch of the dominant kernel, if captured")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,189 @@
+/*
+ * spc5cuda.h -- C ABI of the B200 (sm_100a) implementation of SPC5's
+ * beta(r,VS) hot path: CSR -> beta(r,VS) conversion and y += A x.
+ *
+ * The arrays are byte-for-byte the reference's SPC5Mat arrays
+ * (src/spc5.hpp:44-62): after conversion rowsSize holds the block-row
+ * pointer (ceil(nrows/r)+1 ints), the headers are packed
+ * {int32 first column, r masks} records of 4 + r*sizeof(mask) bytes (mask =
+ * uint8 for double, VS = 8; uint16 for float, VS = 16), and the values are in
+ * block order (sub-row 0 of a block, then sub-row 1, ...).
+ *
+ * All pointers passed to the compute entry points are DEVICE pointers
+ * (cudaMalloc, cudaMallocAsync or torch allocations) with at least 16-byte
+ * alignment for the header and value arrays; work is enqueued on the given
+ * stream (NULL = legacy default stream) and is asynchronous unless stated.
+ * No entry point falls back to the CPU.
+ *
+ * Results: the FP64 and FP32 kernels compute every row in the order of the
+ * reference's AVX-512 kernels (spc5.hpp:2309-2715, default non-MHSUM build),
+ * so y matches the reference bit for bit for finite x.  Unlike the
+ * reference, x is read only at columns present in the matrix (no
+ * SPC5_VEC_PADDING_X needed) and only rows < nbRows of y are written (no
+ * SPC5_VEC_PADDING_Y needed); padded buffers work as well.
+ */
+#ifndef SPC5CUDA_H
+#define SPC5CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SPC5CUDA_API __attribute__((visibility("default")))
+#else
+#define SPC5CUDA_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Format ids: the numbering of SPC5_MATRIX_TYPE (spc5.hpp:17-24). */
+enum spc5cuda_format {
+    SPC5CUDA_UNDEFINED_FORMAT = 0,
+    SPC5CUDA_FORMAT_CSR = 1,
+    SPC5CUDA_FORMAT_1rVc_WT = 2,
+    SPC5CUDA_FORMAT_2rVc = 3,
+    SPC5CUDA_FORMAT_4rVc = 4,
+    SPC5CUDA_FORMAT_8rVc = 5
+};
+
+/* Value types of a matrix: SPC5Mat<double> (VS = 8) or SPC5Mat<float> (VS = 16). */
+enum spc5cuda_value_type { SPC5CUDA_F64 = 0, SPC5CUDA_F32 = 1 };
+
+/* Status codes (the reference throws std::invalid_argument for an unknown
+ * format, spc5.hpp:1014; errors never cross this ABI as exceptions). */
+typedef int spc5cuda_status;
+#define SPC5CUDA_OK 0
+#define SPC5CUDA_ERR_INVALID 1     /* bad argument, size or alignment      */
+#define SPC5CUDA_ERR_CUDA 2        /* a CUDA runtime call failed           */
+#define SPC5CUDA_ERR_NOMEM 3       /* device allocation failed             */
+#define SPC5CUDA_ERR_FORMAT 4      /* unknown format / wrong matrix state  */
+#define SPC5CUDA_ERR_UNSUPPORTED 5 /* valid request this build cannot run  */
+#define SPC5CUDA_ERR_TIMEOUT 6     /* a bounded device wait gave up        */
+#define SPC5CUDA_ERR_DEVICE 7      /* a kernel reported a data error       */
+
+SPC5CUDA_API const char* spc5cuda_status_string(spc5cuda_status s);
+
+/* Status of the last void drop-in call (core_SPC5_*) on this host thread. */
+SPC5CUDA_API spc5cuda_status spc5cuda_get_last_error(void);
+
+/* Stream used by the void drop-in entry points on this host thread
+ * (default NULL = legacy default stream). */
+SPC5CUDA_API void spc5cuda_set_stream(void* stream);
+
+/* ------------------------------------------------------------------------
+ * Drop-in kernels.  Same names, argument order and meaning as the
+ * reference's extern "C" kernels, over device pointers:
+ *   core_SPC5_1rVc_Spmv_{double,float}  spc5.hpp:516-523
+ *   core_SPC5_2rVc_Spmv_{double,float}  spc5.hpp:641-648
+ *   core_SPC5_4rVc_Spmv_{double,float}  spc5.hpp:769-776
+ *   core_SPC5_8rVc_Spmv_{double,float}  spc5.hpp:895-902
+ * y[0..nbRows) += A x.  The value offset of every block-row is not stored
+ * in the format, so each call first derives it from the headers (one extra
+ * pass over the header array, stream-ordered scratch of ceil(nbRows/r)+1
+ * ints from cudaMallocAsync).  The handle API below keeps it resident.
+ * Errors: spc5cuda_get_last_error().
+ * ---------------------------------------------------------------------- */
+SPC5CUDA_API void core_SPC5_1rVc_Spmv_double(const long int nbRows, const int* rowsSizes,
+                                const unsigned char* blocksColumnIndexesWithMasks,
+                                const double* values, const double* x, double* y);
+SPC5CUDA_API void core_SPC5_2rVc_Spmv_double(const long int nbRows, const int* rowsSizes,
+                                const unsigned char* blocksColumnIndexesWithMasks,
+                                const double* values, const double* x, double* y);
+SPC5CUDA_API void core_SPC5_4rVc_Spmv_double(const long int nbRows, const int* rowsSizes,
+                                const unsigned char* blocksColumnIndexesWithMasks,
+                                const double* values, const double* x, double* y);
+SPC5CUDA_API void core_SPC5_8rVc_Spmv_double(const long int nbRows, const int* rowsSizes,
+                                const unsigned char* blocksColumnIndexesWithMasks,
+                                const double* values, const double* x, double* y);
+SPC5CUDA_API void core_SPC5_1rVc_Spmv_float(const long int nbRows, const int* rowsSizes,
+                               const unsigned char* blocksColumnIndexesWithMasks,
+                               const float* values, const float* x, float* y);
+SPC5CUDA_API void core_SPC5_2rVc_Spmv_float(const long int nbRows, const int* rowsSizes,
+                               const unsigned char* blocksColumnIndexesWithMasks,
+                               const float* values, const float* x, float* y);
+SPC5CUDA_API void core_SPC5_4rVc_Spmv_float(const long int nbRows, const int* rowsSizes,
+                               const unsigned char* blocksColumnIndexesWithMasks,
+                               const float* values, const float* x, float* y);
+SPC5CUDA_API void core_SPC5_8rVc_Spmv_float(const long int nbRows, const int* rowsSizes,
+                               const unsigned char* blocksColumnIndexesWithMasks,
+                               const float* values, const float* x, float* y);
+
+/* The same drop-in with an explicit r, stream and status (r in {1,2,4,8}). */
+SPC5CUDA_API spc5cuda_status spc5cuda_core_spmv_f64(int r, long nbRows, const int* rowsSizes,
+                                       const unsigned char* headers, const double* values,
+                                       const double* x, double* y, void* stream);
+SPC5CUDA_API spc5cuda_status spc5cuda_core_spmv_f32(int r, long nbRows, const int* rowsSizes,
+                                       const unsigned char* headers, const float* values,
+                                       const float* x, float* y, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Matrix handle: the device-resident counterpart of SPC5Mat<T>
+ * (spc5.hpp:44-62) plus the precomputed partition that replaces the OpenMP
+ * ThreadInterval split (spc5.hpp:331-427).
+ * ---------------------------------------------------------------------- */
+typedef struct spc5cuda_mat spc5cuda_mat;
+
+typedef struct spc5cuda_info {
+    int value_type;   /* SPC5CUDA_F64 / SPC5CUDA_F32                        */
+    int format;       /* spc5cuda_format                                    */
+    int r;            /* rows per block (0 while CSR)                       */
+    int vs;           /* columns per block: 8 (f64) or 16 (f32)             */
+    int nrows, ncols;
+    long nnz;
+    long nblocks;     /* numberOfBlocks (0 while CSR)                       */
+    long header_bytes;/* nblocks * (4 + r * mask bytes)                     */
+    long device_bytes;/* bytes of device memory held by the handle          */
+} spc5cuda_info;
+
+/* CSR -> handle (the reference builds CSR with COO_sorted_to_CSR,
+ * spc5.hpp:77-104).  Column indices must be sorted inside each row (the
+ * greedy conversion assumes it, like the reference).  values are of the
+ * handle's value type.  on_device != 0: the three arrays are device
+ * pointers; else host pointers (copied).  The call synchronises stream. */
+SPC5CUDA_API spc5cuda_status spc5cuda_mat_create_csr(spc5cuda_mat** out, int value_type, int nrows,
+                                        int ncols, long nnz, const int* rowptr,
+                                        const int* colidx, const void* values, int on_device,
+                                        void* stream);
+
+/* Already-converted beta arrays -> handle (e.g. from a host SPC5Mat after
+ * CSR_to_SPC5).  rowsSize holds ceil(nrows/r)+1 ints. */
+SPC5CUDA_API spc5cuda_status spc5cuda_mat_create_beta(spc5cuda_mat** out, int value_type, int r, int nrows,
+                                         int ncols, long nnz, long nblocks, const int* rowsSize,
+                                         const unsigned char* headers, const void* values,
+                                         int on_device, void* stream);
+
+SPC5CUDA_API spc5cuda_status spc5cuda_mat_destroy(spc5cuda_mat* mat);
+SPC5CUDA_API spc5cuda_status spc5cuda_mat_info(const spc5cuda_mat* mat, spc5cuda_info* out);
+
+/* SPC5_{r}rVc_block_count (spc5.hpp:510-513, 635-638, 764-767, 890-893):
+ * number of blocks the conversion to r would produce.  CSR handles only.
+ * Synchronises stream. */
+SPC5CUDA_API spc5cuda_status spc5cuda_block_count(const spc5cuda_mat* mat, int r, long* nblocks, void* stream);
+
+/* CSR_to_SPC5 (spc5.hpp:989-1018) on the device: converts a CSR handle in
+ * place to format (2..5); the arrays equal the reference's bit for bit.
+ * Synchronises stream (the block count sizes the header allocation). */
+SPC5CUDA_API spc5cuda_status spc5cuda_convert(spc5cuda_mat* mat, int format, void* stream);
+
+/* Copy the converted arrays out (SPC5Mat::rowsSize / blocksColumnIndexesWithMasks
+ * / values).  to_host != 0: host destinations, synchronous. */
+SPC5CUDA_API spc5cuda_status spc5cuda_get_arrays(const spc5cuda_mat* mat, int* rowsSize,
+                                    unsigned char* headers, void* values, int to_host,
+                                    void* stream);
+
+/* SPC5_Spmv (spc5.hpp:1064-1088): y += A x, device x (ncols) and y (nrows)
+ * of the handle's value type. */
+SPC5CUDA_API spc5cuda_status spc5cuda_spmv(const spc5cuda_mat* mat, const void* x, void* y, void* stream);
+
+/* Mixed precision (no counterpart in the reference): an F32 handle, float
+ * x, double y; FP64 per-lane accumulation and FP64 row reduction. */
+SPC5CUDA_API spc5cuda_status spc5cuda_spmv_mixed(const spc5cuda_mat* mat, const float* x, double* y,
+                                    void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPC5CUDA_H */

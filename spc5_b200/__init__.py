@@ -1,0 +1,323 @@
+"""spc5_b200 -- SPC5's beta(r,VS) SpMV hot path on B200 (sm_100a).
+
+Python mirror of the reference's operator interface (src/spc5.hpp) over the
+C ABI of ``libspc5cuda.so`` (include/spc5cuda.h).  The names follow the
+reference: ``SPC5Mat``, ``CSR_to_SPC5``, ``SPC5_Spmv``, ``SPC5_block_count``,
+``SPC5_find_best``, ``core_SPC5_{r}rVc_Spmv_{double,float}``.  Vectors are
+torch CUDA tensors (plumbing only: device memory and the current stream); all
+compute runs in the hand-written CUDA kernels of ``csrc/``.  There is no CPU
+fallback: if the library is missing, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libspc5cuda.so")
+
+# SPC5_MATRIX_TYPE (spc5.hpp:17-24)
+UNDEFINED_FORMAT = 0
+FORMAT_CSR = 1
+FORMAT_1rVc_WT = 2
+FORMAT_2rVc = 3
+FORMAT_4rVc = 4
+FORMAT_8rVc = 5
+FORMAT_OF_R = {1: FORMAT_1rVc_WT, 2: FORMAT_2rVc, 4: FORMAT_4rVc, 8: FORMAT_8rVc}
+R_OF_FORMAT = {v: k for k, v in FORMAT_OF_R.items()}
+
+# SPC5_VEC_PADDING (spc5.hpp:26-29): not needed by these kernels, kept for callers
+SPC5_VEC_PADDING_X = 15
+SPC5_VEC_PADDING_Y = 7
+
+F64 = 0
+F32 = 1
+
+EXPORTED_SYMBOLS = [
+    "spc5cuda_status_string", "spc5cuda_get_last_error", "spc5cuda_set_stream",
+    "core_SPC5_1rVc_Spmv_double", "core_SPC5_2rVc_Spmv_double", "core_SPC5_4rVc_Spmv_double",
+    "core_SPC5_8rVc_Spmv_double", "core_SPC5_1rVc_Spmv_float", "core_SPC5_2rVc_Spmv_float",
+    "core_SPC5_4rVc_Spmv_float", "core_SPC5_8rVc_Spmv_float",
+    "spc5cuda_core_spmv_f64", "spc5cuda_core_spmv_f32",
+    "spc5cuda_mat_create_csr", "spc5cuda_mat_create_beta", "spc5cuda_mat_destroy",
+    "spc5cuda_mat_info", "spc5cuda_block_count", "spc5cuda_convert", "spc5cuda_get_arrays",
+    "spc5cuda_spmv", "spc5cuda_spmv_mixed",
+]
+
+
+class SPC5Error(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        msg = _lib().spc5cuda_status_string(status).decode() if _LIB is not None else str(status)
+        super().__init__(f"{what}: {msg} (status {status})" if what else msg)
+
+
+class spc5cuda_info(C.Structure):
+    _fields_ = [("value_type", C.c_int), ("format", C.c_int), ("r", C.c_int), ("vs", C.c_int),
+                ("nrows", C.c_int), ("ncols", C.c_int), ("nnz", C.c_long), ("nblocks", C.c_long),
+                ("header_bytes", C.c_long), ("device_bytes", C.c_long)]
+
+
+_LIB = None
+_P = C.c_void_p
+_I = C.c_int
+_L = C.c_long
+
+
+def _lib():
+    """Load libspc5cuda.so; raises if the CUDA library was not built."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m spc5_b200.build` "
+                               "(there is no CPU fallback)")
+        lib = C.CDLL(LIB_PATH)
+        lib.spc5cuda_status_string.restype = C.c_char_p
+        lib.spc5cuda_status_string.argtypes = [_I]
+        lib.spc5cuda_get_last_error.restype = _I
+        lib.spc5cuda_set_stream.restype = None
+        lib.spc5cuda_set_stream.argtypes = [_P]
+        for t in ("double", "float"):
+            for r in (1, 2, 4, 8):
+                f = getattr(lib, f"core_SPC5_{r}rVc_Spmv_{t}")
+                f.restype = None
+                f.argtypes = [_L, _P, _P, _P, _P, _P]
+        for n in ("spc5cuda_core_spmv_f64", "spc5cuda_core_spmv_f32"):
+            getattr(lib, n).restype = _I
+            getattr(lib, n).argtypes = [_I, _L, _P, _P, _P, _P, _P, _P]
+        lib.spc5cuda_mat_create_csr.restype = _I
+        lib.spc5cuda_mat_create_csr.argtypes = [C.POINTER(_P), _I, _I, _I, _L, _P, _P, _P, _I, _P]
+        lib.spc5cuda_mat_create_beta.restype = _I
+        lib.spc5cuda_mat_create_beta.argtypes = [C.POINTER(_P), _I, _I, _I, _I, _L, _L, _P, _P, _P,
+                                                 _I, _P]
+        lib.spc5cuda_mat_destroy.restype = _I
+        lib.spc5cuda_mat_destroy.argtypes = [_P]
+        lib.spc5cuda_mat_info.restype = _I
+        lib.spc5cuda_mat_info.argtypes = [_P, C.POINTER(spc5cuda_info)]
+        lib.spc5cuda_block_count.restype = _I
+        lib.spc5cuda_block_count.argtypes = [_P, _I, C.POINTER(_L), _P]
+        lib.spc5cuda_convert.restype = _I
+        lib.spc5cuda_convert.argtypes = [_P, _I, _P]
+        lib.spc5cuda_get_arrays.restype = _I
+        lib.spc5cuda_get_arrays.argtypes = [_P, _P, _P, _P, _I, _P]
+        lib.spc5cuda_spmv.restype = _I
+        lib.spc5cuda_spmv.argtypes = [_P, _P, _P, _P]
+        lib.spc5cuda_spmv_mixed.restype = _I
+        lib.spc5cuda_spmv_mixed.argtypes = [_P, _P, _P, _P]
+        _LIB = lib
+    return _LIB
+
+
+def lib():
+    return _lib()
+
+
+def _check(status: int, what: str = "") -> None:
+    if status != 0:
+        raise SPC5Error(status, what)
+
+
+def _stream(stream=None):
+    import torch
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream)
+
+
+def _dptr(t, dtype=None, what="tensor"):
+    """Device pointer of a contiguous CUDA tensor (checked)."""
+    import torch
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{what} must be a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError(f"{what} must be contiguous")
+    if dtype is not None and t.dtype != dtype:
+        raise TypeError(f"{what} must be {dtype}, got {t.dtype}")
+    return C.c_void_p(t.data_ptr())
+
+
+def _np_ptr(a):
+    return a.ctypes.data_as(_P)
+
+
+def _value_type(dtype) -> int:
+    dt = np.dtype(dtype)
+    if dt == np.float64:
+        return F64
+    if dt == np.float32:
+        return F32
+    raise TypeError(f"unsupported value dtype {dt}")
+
+
+class SPC5Mat:
+    """Device-resident counterpart of the reference's ``SPC5Mat<T>``
+    (spc5.hpp:44-62).  Build one with :func:`csr_matrix` (or
+    :func:`beta_matrix`), convert it in place with :func:`CSR_to_SPC5`."""
+
+    def __init__(self, handle, keep=None):
+        self._h = handle
+        self._keep = keep
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _LIB is not None:
+            _LIB.spc5cuda_mat_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self) -> spc5cuda_info:
+        inf = spc5cuda_info()
+        _check(_lib().spc5cuda_mat_info(self._h, C.byref(inf)), "spc5cuda_mat_info")
+        return inf
+
+    @property
+    def format(self) -> int:
+        return self.info().format
+
+    @property
+    def r(self) -> int:
+        return self.info().r
+
+    @property
+    def numberOfRows(self) -> int:
+        return self.info().nrows
+
+    @property
+    def numberOfColumns(self) -> int:
+        return self.info().ncols
+
+    @property
+    def numberOfNNZ(self) -> int:
+        return self.info().nnz
+
+    @property
+    def numberOfBlocks(self) -> int:
+        return self.info().nblocks
+
+    @property
+    def dtype(self):
+        return np.float64 if self.info().value_type == F64 else np.float32
+
+    def arrays(self):
+        """Host copies of (rowsSize, blocksColumnIndexesWithMasks, values)."""
+        inf = self.info()
+        if inf.r == 0:
+            raise SPC5Error(4, "arrays(): matrix is not converted")
+        nbr = (inf.nrows + inf.r - 1) // inf.r
+        brptr = np.zeros(nbr + 1, dtype=np.int32)
+        headers = np.zeros(inf.header_bytes, dtype=np.uint8)
+        values = np.zeros(inf.nnz, dtype=np.float64 if inf.value_type == F64 else np.float32)
+        _check(_lib().spc5cuda_get_arrays(self._h, _np_ptr(brptr), _np_ptr(headers), _np_ptr(values),
+                                          1, None), "spc5cuda_get_arrays")
+        return brptr, headers, values
+
+
+def csr_matrix(rowptr, colidx, values, ncols: int, dtype=None, stream=None) -> SPC5Mat:
+    """A CSR ``SPC5Mat`` from host numpy arrays or CUDA tensors (int32
+    indices, sorted columns per row).  ``dtype`` (float64/float32) casts the
+    values; float32 gives the VS = 16 layout used by the float and mixed
+    kernels."""
+    import torch
+    on_device = isinstance(rowptr, torch.Tensor) and rowptr.is_cuda
+    if on_device:
+        vals = values if dtype is None else values.to(getattr(torch, np.dtype(dtype).name))
+        vt = _value_type(np.float64 if vals.dtype == torch.float64 else np.float32)
+        nrows = rowptr.numel() - 1
+        nnz = colidx.numel()
+        ptrs = (_dptr(rowptr, torch.int32, "rowptr"), _dptr(colidx, torch.int32, "colidx"),
+                _dptr(vals, None, "values"))
+        keep = (rowptr, colidx, vals)
+    else:
+        rp = np.ascontiguousarray(rowptr, dtype=np.int32)
+        ci = np.ascontiguousarray(colidx, dtype=np.int32)
+        vals = np.ascontiguousarray(values, dtype=dtype if dtype is not None else None)
+        vt = _value_type(vals.dtype)
+        nrows = len(rp) - 1
+        nnz = len(ci)
+        ptrs = (_np_ptr(rp), _np_ptr(ci), _np_ptr(vals))
+        keep = (rp, ci, vals)
+    h = C.c_void_p()
+    st = _stream(stream) if torch.cuda.is_available() else None
+    _check(_lib().spc5cuda_mat_create_csr(C.byref(h), vt, nrows, int(ncols), nnz, *ptrs,
+                                          1 if on_device else 0, st), "spc5cuda_mat_create_csr")
+    del keep
+    return SPC5Mat(h)
+
+
+def beta_matrix(r: int, nrows: int, ncols: int, rowsSize, headers, values, stream=None) -> SPC5Mat:
+    """An ``SPC5Mat`` from already-converted host arrays (e.g. the reference's
+    ``SPC5Mat`` after ``CSR_to_SPC5``)."""
+    brptr = np.ascontiguousarray(rowsSize, dtype=np.int32)
+    hdr = np.ascontiguousarray(headers, dtype=np.uint8)
+    vals = np.ascontiguousarray(values)
+    vt = _value_type(vals.dtype)
+    stride = 4 + r * (1 if vt == F64 else 2)
+    if len(hdr) % stride:
+        raise ValueError("header array size is not a multiple of the block stride")
+    h = C.c_void_p()
+    _check(_lib().spc5cuda_mat_create_beta(C.byref(h), vt, r, nrows, ncols, len(vals), len(hdr) // stride,
+                                           _np_ptr(brptr), _np_ptr(hdr), _np_ptr(vals), 0,
+                                           _stream(stream)), "spc5cuda_mat_create_beta")
+    return SPC5Mat(h)
+
+
+def SPC5_block_count(mat: SPC5Mat, fmt: int, stream=None) -> int:
+    """Block count of converting ``mat`` (CSR) to ``fmt``; the reference's
+    wrapper (spc5.hpp:1120-1148) computes it and drops it, this returns it."""
+    r = R_OF_FORMAT.get(fmt)
+    if r is None:
+        raise SPC5Error(4, "SPC5_block_count : Unknown format type")
+    out = C.c_long(0)
+    _check(_lib().spc5cuda_block_count(mat.handle, r, C.byref(out), _stream(stream)),
+           "spc5cuda_block_count")
+    return int(out.value)
+
+
+def CSR_to_SPC5(mat: SPC5Mat, fmt: int, stream=None) -> None:
+    """In-place conversion on the device (CSR_to_SPC5, spc5.hpp:989-1018)."""
+    _check(_lib().spc5cuda_convert(mat.handle, int(fmt), _stream(stream)), "CSR_to_SPC5")
+
+
+def SPC5_Spmv(mat: SPC5Mat, x, y, stream=None) -> None:
+    """y += A x (SPC5_Spmv, spc5.hpp:1064-1088); x, y CUDA tensors of the
+    matrix's value type."""
+    import torch
+    dt = torch.float64 if mat.dtype == np.float64 else torch.float32
+    _check(_lib().spc5cuda_spmv(mat.handle, _dptr(x, dt, "x"), _dptr(y, dt, "y"), _stream(stream)),
+           "SPC5_Spmv")
+
+
+def SPC5_Spmv_mixed(mat: SPC5Mat, x, y, stream=None) -> None:
+    """y += A x with FP32 values and x, FP64 accumulation and y."""
+    import torch
+    _check(_lib().spc5cuda_spmv_mixed(mat.handle, _dptr(x, torch.float32, "x"),
+                                      _dptr(y, torch.float64, "y"), _stream(stream)), "SPC5_Spmv_mixed")
+
+
+def core_spmv(r: int, nbRows: int, rowsSizes, headers, values, x, y, stream=None) -> None:
+    """The drop-in kernel ``core_SPC5_{r}rVc_Spmv_{double,float}`` over device
+    tensors, through its explicit-stream C entry point."""
+    import torch
+    f = _lib().spc5cuda_core_spmv_f64 if values.dtype == torch.float64 else _lib().spc5cuda_core_spmv_f32
+    _check(f(int(r), int(nbRows), _dptr(rowsSizes, torch.int32, "rowsSizes"),
+             _dptr(headers, torch.uint8, "headers"), _dptr(values, None, "values"),
+             _dptr(x, values.dtype, "x"), _dptr(y, values.dtype, "y"), _stream(stream)),
+           f"core_SPC5_{r}rVc_Spmv")
+
+
+def core_spmv_void(r: int, nbRows: int, rowsSizes, headers, values, x, y, stream=None) -> None:
+    """Calls the exact reference-named void symbol ``core_SPC5_{r}rVc_Spmv_{T}``
+    (stream from ``spc5cuda_set_stream``) and checks ``spc5cuda_get_last_error``."""
+    import torch
+    t = "double" if values.dtype == torch.float64 else "float"
+    lib_ = _lib()
+    lib_.spc5cuda_set_stream(_stream(stream))
+    getattr(lib_, f"core_SPC5_{r}rVc_Spmv_{t}")(int(nbRows), _dptr(rowsSizes, torch.int32),
+                                                 _dptr(headers, torch.uint8), _dptr(values),
+                                                 _dptr(x, values.dtype), _dptr(y, values.dtype))
+    _check(lib_.spc5cuda_get_last_error(), f"core_SPC5_{r}rVc_Spmv_{t}")

@@ -1,0 +1,469 @@
+// capi.cu -- the C ABI (include/spc5cuda.h): matrix handles, device
+// conversion, drop-in kernels.  Every entry point catches the internal
+// spc5cuda::Error and returns a status code; nothing throws across the ABI.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace spc5cuda {
+
+int sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
+    SPC5_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (cached[dev] == 0) {
+        int n = 0;
+        SPC5_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+        cached[dev] = n > 0 ? n : 1;
+    }
+    return cached[dev];
+}
+
+namespace {
+
+thread_local spc5cuda_status g_last_error = SPC5CUDA_OK;
+thread_local cudaStream_t g_stream = nullptr;
+
+// Stream-ordered device buffer (cudaMallocAsync / cudaFreeAsync).
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaStream_t s = nullptr;
+    DevBuf() = default;
+    DevBuf(size_t n, cudaStream_t st) : bytes(n), s(st) {
+        if (n) SPC5_CUDA(cudaMallocAsync(&p, n, st));
+    }
+    ~DevBuf() {
+        if (p) cudaFreeAsync(p, s);
+    }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+// Persistent device buffer owned by a matrix handle.
+struct Owned {
+    void* p = nullptr;
+    size_t bytes = 0;
+    void alloc(size_t n) {
+        release();
+        if (n) SPC5_CUDA(cudaMalloc(&p, n));
+        bytes = n;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    ~Owned() { release(); }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+bool aligned(const void* p, size_t a) { return (reinterpret_cast<uintptr_t>(p) % a) == 0; }
+
+int format_to_r(int format) {
+    switch (format) {
+        case SPC5CUDA_FORMAT_1rVc_WT: return 1;
+        case SPC5CUDA_FORMAT_2rVc: return 2;
+        case SPC5CUDA_FORMAT_4rVc: return 4;
+        case SPC5CUDA_FORMAT_8rVc: return 8;
+        default: return 0;
+    }
+}
+
+int r_to_format(int r) {
+    switch (r) {
+        case 1: return SPC5CUDA_FORMAT_1rVc_WT;
+        case 2: return SPC5CUDA_FORMAT_2rVc;
+        case 4: return SPC5CUDA_FORMAT_4rVc;
+        case 8: return SPC5CUDA_FORMAT_8rVc;
+        default: return SPC5CUDA_UNDEFINED_FORMAT;
+    }
+}
+
+int vs_of(int value_type) { return value_type == SPC5CUDA_F64 ? 8 : 16; }
+int mask_bytes_of(int value_type) { return value_type == SPC5CUDA_F64 ? 1 : 2; }
+int value_bytes_of(int value_type) { return value_type == SPC5CUDA_F64 ? 8 : 4; }
+
+template <class F>
+spc5cuda_status guarded(F&& f) {
+    try {
+        f();
+        return SPC5CUDA_OK;
+    } catch (const Error& e) {
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        return SPC5CUDA_ERR_NOMEM;
+    } catch (...) {
+        return SPC5CUDA_ERR_INVALID;
+    }
+}
+
+void require(bool cond, spc5cuda_status s, const char* what) {
+    if (!cond) throw Error(s, what);
+}
+
+}  // namespace
+}  // namespace spc5cuda
+
+using namespace spc5cuda;
+
+// The device-resident SPC5Mat<T> (src/spc5.hpp:44-62).
+struct spc5cuda_mat {
+    int value_type = SPC5CUDA_F64;
+    int format = SPC5CUDA_UNDEFINED_FORMAT;
+    int r = 0;
+    int nrows = 0, ncols = 0;
+    long nnz = 0;
+    long nblocks = 0;
+    Owned rowptr;   // CSR row pointer (nrows+1); dropped after conversion
+    Owned colidx;   // CSR column indices; dropped after conversion
+    Owned values;   // nnz values (CSR order, then beta order)
+    Owned brptr;    // rowsSize after conversion: ceil(nrows/r)+1 block offsets
+    Owned headers;  // blocksColumnIndexesWithMasks
+    Owned valptr;   // ceil(nrows/r)+1 value offsets (not in the reference format)
+
+    int nbr() const { return r ? div_up(nrows, r) : 0; }
+    BetaView view() const {
+        BetaView v;
+        v.r = r;
+        v.nrows = nrows;
+        v.nbr = nbr();
+        v.brptr = brptr.as<int>();
+        v.headers = headers.as<uint8_t>();
+        v.values = values.p;
+        v.valptr = valptr.as<int>();
+        return v;
+    }
+    long device_bytes() const {
+        return long(rowptr.bytes + colidx.bytes + values.bytes + brptr.bytes + headers.bytes +
+                    valptr.bytes);
+    }
+};
+
+namespace {
+
+void copy_in(Owned& dst, const void* src, size_t bytes, int on_device, cudaStream_t s) {
+    dst.alloc(bytes);
+    if (bytes)
+        SPC5_CUDA(cudaMemcpyAsync(dst.p, src, bytes,
+                                  on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+}
+
+// Runs the validation kernel and turns its flag into a status.
+void validate_csr(const spc5cuda_mat* m, cudaStream_t s) {
+    DevBuf flag(sizeof(int), s);
+    launch_validate_csr(m->nrows, m->ncols, m->nnz, m->rowptr.as<int>(), m->colidx.as<int>(),
+                        flag.as<int>(), s);
+    int h = 0;
+    SPC5_CUDA(cudaMemcpyAsync(&h, flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SPC5_CUDA(cudaStreamSynchronize(s));
+    if (h != 0) throw Error(SPC5CUDA_ERR_INVALID, "malformed CSR");
+}
+
+// Block counts per block-row -> exclusive scan into brptr; returns the total.
+long count_blocks(const spc5cuda_mat* m, int r, int* brptr_out, cudaStream_t s) {
+    const long nbr = div_up(m->nrows, r);
+    DevBuf tmp(sizeof(int) * size_t(scan_tmp_ints(nbr) + 1), s);
+    launch_blockrow_counts(vs_of(m->value_type), r, m->nrows, m->rowptr.as<int>(),
+                           m->colidx.as<int>(), brptr_out, s);
+    exclusive_scan_i32(brptr_out, brptr_out, nbr, tmp.as<int>(), s);
+    int total = 0;
+    SPC5_CUDA(cudaMemcpyAsync(&total, brptr_out + nbr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SPC5_CUDA(cudaStreamSynchronize(s));
+    return total;
+}
+
+// Value offsets of every block-row from the header masks.
+void valptr_from_headers(int mask_bytes, int r, int nbr, const int* brptr, const uint8_t* headers,
+                         int* valptr, cudaStream_t s) {
+    DevBuf tmp(sizeof(int) * size_t(scan_tmp_ints(nbr) + 1), s);
+    launch_blockrow_value_counts(mask_bytes, r, nbr, brptr, headers, valptr, s);
+    exclusive_scan_i32(valptr, valptr, nbr, tmp.as<int>(), s);
+}
+
+template <class T>
+void core_spmv(int r, long nbRows, const int* rowsSizes, const unsigned char* headers,
+               const T* values, const T* x, T* y, cudaStream_t s) {
+    require(r == 1 || r == 2 || r == 4 || r == 8, SPC5CUDA_ERR_FORMAT, "r must be 1, 2, 4 or 8");
+    require(nbRows >= 0 && nbRows < (1L << 31), SPC5CUDA_ERR_INVALID, "nbRows out of range");
+    if (nbRows == 0) return;
+    require(rowsSizes && headers && values && x && y, SPC5CUDA_ERR_INVALID, "null pointer");
+    require(aligned(headers, 4) && aligned(values, sizeof(T)), SPC5CUDA_ERR_INVALID,
+            "misaligned array");
+    const int nbr = div_up(nbRows, r);
+    DevBuf valptr(sizeof(int) * size_t(nbr + 1), s);
+    valptr_from_headers(sizeof(T) == 8 ? 1 : 2, r, nbr, rowsSizes, headers, valptr.as<int>(), s);
+    BetaView v;
+    v.r = r;
+    v.nrows = int(nbRows);
+    v.nbr = nbr;
+    v.brptr = rowsSizes;
+    v.headers = headers;
+    v.values = values;
+    v.valptr = valptr.as<int>();
+    if constexpr (sizeof(T) == 8)
+        launch_spmv_f64(v, x, y, s);
+    else
+        launch_spmv_f32(v, x, y, s);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* spc5cuda_status_string(spc5cuda_status s) {
+    switch (s) {
+        case SPC5CUDA_OK: return "ok";
+        case SPC5CUDA_ERR_INVALID: return "invalid argument";
+        case SPC5CUDA_ERR_CUDA: return "CUDA error";
+        case SPC5CUDA_ERR_NOMEM: return "out of device memory";
+        case SPC5CUDA_ERR_FORMAT: return "unknown format or wrong matrix state";
+        case SPC5CUDA_ERR_UNSUPPORTED: return "unsupported";
+        case SPC5CUDA_ERR_TIMEOUT: return "device wait timed out";
+        case SPC5CUDA_ERR_DEVICE: return "device reported a data error";
+        default: return "unknown status";
+    }
+}
+
+spc5cuda_status spc5cuda_get_last_error(void) { return g_last_error; }
+
+void spc5cuda_set_stream(void* stream) { g_stream = static_cast<cudaStream_t>(stream); }
+
+spc5cuda_status spc5cuda_core_spmv_f64(int r, long nbRows, const int* rowsSizes,
+                                       const unsigned char* headers, const double* values,
+                                       const double* x, double* y, void* stream) {
+    return guarded([&] {
+        core_spmv<double>(r, nbRows, rowsSizes, headers, values, x, y,
+                          static_cast<cudaStream_t>(stream));
+    });
+}
+
+spc5cuda_status spc5cuda_core_spmv_f32(int r, long nbRows, const int* rowsSizes,
+                                       const unsigned char* headers, const float* values,
+                                       const float* x, float* y, void* stream) {
+    return guarded([&] {
+        core_spmv<float>(r, nbRows, rowsSizes, headers, values, x, y,
+                         static_cast<cudaStream_t>(stream));
+    });
+}
+
+#define SPC5_DROPIN(R_, NAME_, T_, FN_)                                                       \
+    void NAME_(const long int nbRows, const int* rowsSizes,                                   \
+               const unsigned char* blocksColumnIndexesWithMasks, const T_* values,           \
+               const T_* x, T_* y) {                                                          \
+        g_last_error =                                                                        \
+            FN_(R_, nbRows, rowsSizes, blocksColumnIndexesWithMasks, values, x, y, g_stream); \
+    }
+
+SPC5_DROPIN(1, core_SPC5_1rVc_Spmv_double, double, spc5cuda_core_spmv_f64)
+SPC5_DROPIN(2, core_SPC5_2rVc_Spmv_double, double, spc5cuda_core_spmv_f64)
+SPC5_DROPIN(4, core_SPC5_4rVc_Spmv_double, double, spc5cuda_core_spmv_f64)
+SPC5_DROPIN(8, core_SPC5_8rVc_Spmv_double, double, spc5cuda_core_spmv_f64)
+SPC5_DROPIN(1, core_SPC5_1rVc_Spmv_float, float, spc5cuda_core_spmv_f32)
+SPC5_DROPIN(2, core_SPC5_2rVc_Spmv_float, float, spc5cuda_core_spmv_f32)
+SPC5_DROPIN(4, core_SPC5_4rVc_Spmv_float, float, spc5cuda_core_spmv_f32)
+SPC5_DROPIN(8, core_SPC5_8rVc_Spmv_float, float, spc5cuda_core_spmv_f32)
+#undef SPC5_DROPIN
+
+spc5cuda_status spc5cuda_mat_create_csr(spc5cuda_mat** out, int value_type, int nrows, int ncols,
+                                        long nnz, const int* rowptr, const int* colidx,
+                                        const void* values, int on_device, void* stream) {
+    return guarded([&] {
+        require(out != nullptr, SPC5CUDA_ERR_INVALID, "null out");
+        *out = nullptr;
+        require(value_type == SPC5CUDA_F64 || value_type == SPC5CUDA_F32, SPC5CUDA_ERR_INVALID,
+                "value type");
+        require(nrows >= 0 && ncols >= 0 && nnz >= 0 && nnz < (1L << 31), SPC5CUDA_ERR_INVALID,
+                "sizes");
+        require(rowptr != nullptr && (nnz == 0 || (colidx && values)), SPC5CUDA_ERR_INVALID,
+                "null array");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        auto* m = new spc5cuda_mat();
+        try {
+            m->value_type = value_type;
+            m->format = SPC5CUDA_FORMAT_CSR;
+            m->nrows = nrows;
+            m->ncols = ncols;
+            m->nnz = nnz;
+            copy_in(m->rowptr, rowptr, sizeof(int) * size_t(nrows + 1), on_device, s);
+            copy_in(m->colidx, colidx, sizeof(int) * size_t(nnz), on_device, s);
+            copy_in(m->values, values, size_t(value_bytes_of(value_type)) * size_t(nnz),
+                    on_device, s);
+            validate_csr(m, s);
+        } catch (...) {
+            delete m;
+            throw;
+        }
+        *out = m;
+    });
+}
+
+spc5cuda_status spc5cuda_mat_create_beta(spc5cuda_mat** out, int value_type, int r, int nrows,
+                                         int ncols, long nnz, long nblocks, const int* rowsSize,
+                                         const unsigned char* headers, const void* values,
+                                         int on_device, void* stream) {
+    return guarded([&] {
+        require(out != nullptr, SPC5CUDA_ERR_INVALID, "null out");
+        *out = nullptr;
+        require(value_type == SPC5CUDA_F64 || value_type == SPC5CUDA_F32, SPC5CUDA_ERR_INVALID,
+                "value type");
+        require(r_to_format(r) != SPC5CUDA_UNDEFINED_FORMAT, SPC5CUDA_ERR_FORMAT, "r");
+        require(nrows >= 0 && ncols >= 0 && nnz >= 0 && nnz < (1L << 31) && nblocks >= 0 &&
+                    nblocks < (1L << 31),
+                SPC5CUDA_ERR_INVALID, "sizes");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        auto* m = new spc5cuda_mat();
+        try {
+            m->value_type = value_type;
+            m->format = r_to_format(r);
+            m->r = r;
+            m->nrows = nrows;
+            m->ncols = ncols;
+            m->nnz = nnz;
+            m->nblocks = nblocks;
+            const int nbr = div_up(nrows, r);
+            const size_t stride = 4 + size_t(r) * mask_bytes_of(value_type);
+            copy_in(m->brptr, rowsSize, sizeof(int) * size_t(nbr + 1), on_device, s);
+            copy_in(m->headers, headers, stride * size_t(nblocks), on_device, s);
+            copy_in(m->values, values, size_t(value_bytes_of(value_type)) * size_t(nnz), on_device,
+                    s);
+            m->valptr.alloc(sizeof(int) * size_t(nbr + 1));
+            if (nbr > 0) {
+                valptr_from_headers(mask_bytes_of(value_type), r, nbr, m->brptr.as<int>(),
+                                    m->headers.as<uint8_t>(), m->valptr.as<int>(), s);
+            } else {
+                SPC5_CUDA(cudaMemsetAsync(m->valptr.p, 0, sizeof(int), s));
+            }
+            SPC5_CUDA(cudaStreamSynchronize(s));
+        } catch (...) {
+            delete m;
+            throw;
+        }
+        *out = m;
+    });
+}
+
+spc5cuda_status spc5cuda_mat_destroy(spc5cuda_mat* mat) {
+    return guarded([&] { delete mat; });
+}
+
+spc5cuda_status spc5cuda_mat_info(const spc5cuda_mat* m, spc5cuda_info* out) {
+    return guarded([&] {
+        require(m && out, SPC5CUDA_ERR_INVALID, "null");
+        out->value_type = m->value_type;
+        out->format = m->format;
+        out->r = m->r;
+        out->vs = vs_of(m->value_type);
+        out->nrows = m->nrows;
+        out->ncols = m->ncols;
+        out->nnz = m->nnz;
+        out->nblocks = m->nblocks;
+        out->header_bytes = m->nblocks * (4 + long(m->r) * mask_bytes_of(m->value_type));
+        out->device_bytes = m->device_bytes();
+    });
+}
+
+spc5cuda_status spc5cuda_block_count(const spc5cuda_mat* m, int r, long* nblocks, void* stream) {
+    return guarded([&] {
+        require(m && nblocks, SPC5CUDA_ERR_INVALID, "null");
+        require(m->format == SPC5CUDA_FORMAT_CSR, SPC5CUDA_ERR_FORMAT, "block count needs CSR");
+        require(r_to_format(r) != SPC5CUDA_UNDEFINED_FORMAT, SPC5CUDA_ERR_FORMAT, "r");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        DevBuf counts(sizeof(int) * size_t(div_up(m->nrows, r) + 1), s);
+        *nblocks = count_blocks(m, r, counts.as<int>(), s);
+    });
+}
+
+spc5cuda_status spc5cuda_convert(spc5cuda_mat* m, int format, void* stream) {
+    return guarded([&] {
+        require(m != nullptr, SPC5CUDA_ERR_INVALID, "null");
+        require(m->format == SPC5CUDA_FORMAT_CSR, SPC5CUDA_ERR_FORMAT, "matrix is not CSR");
+        const int r = format_to_r(format);
+        require(r != 0, SPC5CUDA_ERR_FORMAT, "CSR_to_SPC5 : Unknown format type");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const int nbr = div_up(m->nrows, r);
+        Owned brptr;
+        brptr.alloc(sizeof(int) * size_t(nbr + 1));
+        const long nb = m->nrows > 0 ? count_blocks(m, r, brptr.as<int>(), s) : 0;
+        if (m->nrows == 0) SPC5_CUDA(cudaMemsetAsync(brptr.p, 0, sizeof(int), s));
+        const size_t stride = 4 + size_t(r) * mask_bytes_of(m->value_type);
+        Owned headers, values, valptr;
+        headers.alloc(stride * size_t(nb));
+        values.alloc(size_t(value_bytes_of(m->value_type)) * size_t(m->nnz));
+        valptr.alloc(sizeof(int) * size_t(nbr + 1));
+        launch_emit(vs_of(m->value_type), r, m->nrows, m->rowptr.as<int>(), m->colidx.as<int>(),
+                    m->values.p, value_bytes_of(m->value_type), brptr.as<int>(),
+                    headers.as<uint8_t>(), values.p, s);
+        launch_valptr_from_csr(r, m->nrows, m->rowptr.as<int>(), valptr.as<int>(), s);
+        SPC5_CUDA(cudaStreamSynchronize(s));
+        std::swap(m->brptr.p, brptr.p);
+        std::swap(m->brptr.bytes, brptr.bytes);
+        std::swap(m->headers.p, headers.p);
+        std::swap(m->headers.bytes, headers.bytes);
+        std::swap(m->values.p, values.p);
+        std::swap(m->values.bytes, values.bytes);
+        std::swap(m->valptr.p, valptr.p);
+        std::swap(m->valptr.bytes, valptr.bytes);
+        m->rowptr.release();
+        m->colidx.release();
+        m->r = r;
+        m->format = format;
+        m->nblocks = nb;
+    });
+}
+
+spc5cuda_status spc5cuda_get_arrays(const spc5cuda_mat* m, int* rowsSize, unsigned char* headers,
+                                    void* values, int to_host, void* stream) {
+    return guarded([&] {
+        require(m != nullptr, SPC5CUDA_ERR_INVALID, "null");
+        require(m->r != 0, SPC5CUDA_ERR_FORMAT, "matrix is not converted");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const cudaMemcpyKind kind = to_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+        if (rowsSize)
+            SPC5_CUDA(cudaMemcpyAsync(rowsSize, m->brptr.p, m->brptr.bytes, kind, s));
+        if (headers && m->headers.bytes)
+            SPC5_CUDA(cudaMemcpyAsync(headers, m->headers.p, m->headers.bytes, kind, s));
+        if (values && m->values.bytes)
+            SPC5_CUDA(cudaMemcpyAsync(values, m->values.p, m->values.bytes, kind, s));
+        if (to_host) SPC5_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+spc5cuda_status spc5cuda_spmv(const spc5cuda_mat* m, const void* x, void* y, void* stream) {
+    return guarded([&] {
+        require(m != nullptr, SPC5CUDA_ERR_INVALID, "null");
+        require(m->r != 0, SPC5CUDA_ERR_FORMAT, "SPC5_Spmv : Unknown format type");
+        if (m->nrows == 0) return;
+        require(x && y, SPC5CUDA_ERR_INVALID, "null vector");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        if (m->value_type == SPC5CUDA_F64)
+            launch_spmv_f64(m->view(), static_cast<const double*>(x), static_cast<double*>(y), s);
+        else
+            launch_spmv_f32(m->view(), static_cast<const float*>(x), static_cast<float*>(y), s);
+    });
+}
+
+spc5cuda_status spc5cuda_spmv_mixed(const spc5cuda_mat* m, const float* x, double* y,
+                                    void* stream) {
+    return guarded([&] {
+        require(m != nullptr, SPC5CUDA_ERR_INVALID, "null");
+        require(m->r != 0, SPC5CUDA_ERR_FORMAT, "matrix is not converted");
+        require(m->value_type == SPC5CUDA_F32, SPC5CUDA_ERR_FORMAT,
+                "mixed precision needs an F32 matrix");
+        if (m->nrows == 0) return;
+        require(x && y, SPC5CUDA_ERR_INVALID, "null vector");
+        launch_spmv_mixed(m->view(), x, y, static_cast<cudaStream_t>(stream));
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,54 @@
+// kernels.h -- host-side launchers of the sm_100a kernels (internal).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace spc5cuda {
+
+// ---- scan ---------------------------------------------------------------
+// out[0..n] = exclusive prefix sum of in[0..n), out[n] = total.  tmp must
+// hold scan_tmp_ints(n) ints.  in and out may alias.
+long scan_tmp_ints(long n);
+void exclusive_scan_i32(const int* in, int* out, long n, int* tmp, cudaStream_t s);
+
+// ---- CSR checks and conversion (convert.cu) -------------------------------
+// Writes 0 to *d_flag when the CSR is well formed (monotone rowptr starting
+// at 0, columns in [0, ncols), strictly increasing inside a row), else an
+// error code (1 rowptr, 2 column range, 3 order/duplicate).
+void launch_validate_csr(int nrows, int ncols, long nnz, const int* rowptr, const int* colidx,
+                         int* d_flag, cudaStream_t s);
+
+// counts[br] = blocks of block-row br for rows-per-block r and VS columns.
+void launch_blockrow_counts(int vs, int r, int nrows, const int* rowptr, const int* colidx,
+                            int* counts, cudaStream_t s);
+
+// Emits headers and reordered values of every block-row (brptr = exclusive
+// scan of the counts).  value_bytes is 8 or 4.
+void launch_emit(int vs, int r, int nrows, const int* rowptr, const int* colidx,
+                 const void* vin, int value_bytes, const int* brptr, uint8_t* headers,
+                 void* vout, cudaStream_t s);
+
+// valptr[br] = rowptr[min(br*r, nrows)] for br in [0, nbr].
+void launch_valptr_from_csr(int r, int nrows, const int* rowptr, int* valptr, cudaStream_t s);
+
+// counts[br] = number of values of block-row br, from the header masks.
+void launch_blockrow_value_counts(int mask_bytes, int r, int nbr, const int* brptr,
+                                  const uint8_t* headers, int* counts, cudaStream_t s);
+
+// ---- SpMV (spmv.cu) ------------------------------------------------------
+struct BetaView {
+    int r;
+    int nrows;
+    int nbr;            // ceil(nrows / r)
+    const int* brptr;   // nbr + 1 block offsets
+    const uint8_t* headers;
+    const void* values;
+    const int* valptr;  // nbr + 1 value offsets
+};
+
+void launch_spmv_f64(const BetaView& m, const double* x, double* y, cudaStream_t s);
+void launch_spmv_f32(const BetaView& m, const float* x, float* y, cudaStream_t s);
+void launch_spmv_mixed(const BetaView& m, const float* x, double* y, cudaStream_t s);
+
+}  // namespace spc5cuda

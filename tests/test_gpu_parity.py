@@ -1,0 +1,210 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and the
+reference's golden outputs.
+
+Bars:
+* conversion (CSR_to_SPC5 on the device): rowsSize, headers and values
+  identical byte for byte to the reference's;
+* FP64 / FP32 SpMV: y identical bit for bit to the reference's AVX-512
+  kernels (finite x), which the oracle restates and golden.npz records;
+* mixed precision: identical to the oracle's definition, and within 1e-6
+  normwise relative error of the FP64 CSR oracle (componentwise error
+  |dy_i| / sum_j |a_ij x_j| <= 2.5e-7, two FP32 roundings of a and x).
+"""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+import spc5_b200 as S
+from spc5_b200 import matrices as M
+
+pytestmark = pytest.mark.gpu
+
+DTYPES = [("f64", np.float64), ("f32", np.float32)]
+TORCH = {np.float64: torch.float64, np.float32: torch.float32}
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def names(golden):
+    return [str(n) for n in golden["names"]]
+
+
+def converted(csr, dt, r):
+    m = S.csr_matrix(csr.rowptr, csr.colidx, csr.values.astype(dt), csr.ncols)
+    S.CSR_to_SPC5(m, S.FORMAT_OF_R[r])
+    return m
+
+
+def gpu_spmv(m, x, y0):
+    y = dev(y0)
+    S.SPC5_Spmv(m, dev(x), y)
+    torch.cuda.synchronize()
+    return y.cpu().numpy()
+
+
+def golden_csr(golden, n):
+    return M.CSR(int(golden[f"{n}/nrows"]), int(golden[f"{n}/ncols"]), golden[f"{n}/rowptr"],
+                 golden[f"{n}/colidx"], golden[f"{n}/values"], n)
+
+
+@pytest.mark.parametrize("tag,dt", DTYPES)
+@pytest.mark.parametrize("r", [1, 2, 4, 8])
+def test_convert_matches_reference(cuda, golden, tag, dt, r):
+    for n in names(golden):
+        csr = golden_csr(golden, n)
+        m = S.csr_matrix(csr.rowptr, csr.colidx, csr.values.astype(dt), csr.ncols)
+        assert S.SPC5_block_count(m, S.FORMAT_OF_R[r]) == int(golden[f"{n}/{tag}/r{r}/block_count"])
+        S.CSR_to_SPC5(m, S.FORMAT_OF_R[r])
+        assert m.format == S.FORMAT_OF_R[r] and m.numberOfBlocks == int(golden[f"{n}/{tag}/r{r}/block_count"])
+        brptr, headers, vals = m.arrays()
+        assert np.array_equal(brptr, golden[f"{n}/{tag}/r{r}/rowsSize"]), n
+        assert np.array_equal(headers, golden[f"{n}/{tag}/r{r}/headers"]), n
+        assert vals.tobytes() == golden[f"{n}/{tag}/r{r}/values"].tobytes(), n
+
+
+@pytest.mark.parametrize("tag,dt", DTYPES)
+@pytest.mark.parametrize("r", [1, 2, 4, 8])
+def test_spmv_matches_reference(cuda, golden, tag, dt, r):
+    for n in names(golden):
+        csr = golden_csr(golden, n)
+        m = converted(csr, dt, r)
+        y = gpu_spmv(m, golden[f"{n}/x"].astype(dt), np.zeros(csr.nrows, dtype=dt))
+        assert y.tobytes() == golden[f"{n}/{tag}/r{r}/y"].tobytes(), n
+
+
+@pytest.mark.parametrize("tag,dt", DTYPES)
+@pytest.mark.parametrize("r", [1, 2, 4, 8])
+def test_dropin_entry_points(cuda, golden, tag, dt, r):
+    """core_SPC5_{r}rVc_Spmv_{T} over the reference's own converted arrays."""
+    for n in names(golden)[:5]:
+        nrows = int(golden[f"{n}/nrows"])
+        args = (dev(golden[f"{n}/{tag}/r{r}/rowsSize"]), dev(golden[f"{n}/{tag}/r{r}/headers"]),
+                dev(golden[f"{n}/{tag}/r{r}/values"]), dev(golden[f"{n}/x"].astype(dt)))
+        for fn in (S.core_spmv, S.core_spmv_void):
+            y = torch.zeros(nrows, dtype=TORCH[dt], device="cuda")
+            fn(r, nrows, *args, y)
+            torch.cuda.synchronize()
+            assert y.cpu().numpy().tobytes() == golden[f"{n}/{tag}/r{r}/y"].tobytes(), (n, fn.__name__)
+
+
+@pytest.mark.parametrize("r", [1, 2, 4, 8])
+def test_handle_from_reference_arrays(cuda, golden, r):
+    for n in names(golden)[:4]:
+        nrows, ncols = int(golden[f"{n}/nrows"]), int(golden[f"{n}/ncols"])
+        m = S.beta_matrix(r, nrows, ncols, golden[f"{n}/f64/r{r}/rowsSize"], golden[f"{n}/f64/r{r}/headers"],
+                          golden[f"{n}/f64/r{r}/values"])
+        y = gpu_spmv(m, golden[f"{n}/x"], np.zeros(nrows))
+        assert y.tobytes() == golden[f"{n}/f64/r{r}/y"].tobytes()
+
+
+def irregular_cases():
+    yield M.random_csr(1000, 1200, 0.02, seed=1, empty_row_frac=0.2)
+    yield M.random_csr(333, 64, 0.5, seed=2)
+    yield M.powerlaw(20000, seed=7)
+    yield M.banded(4099, 150, 0.1, seed=8)
+    yield M.stencil27(9)
+    yield M.from_coo(5, 3, [0, 2, 4], [2, 0, 1], [1.5, -2.0, 3.25])  # ncols < VS
+    yield M.from_coo(7, 7, [], [], [])  # no entries at all
+    yield M.dense(40)
+
+
+@pytest.mark.parametrize("tag,dt", DTYPES)
+@pytest.mark.parametrize("r", [1, 2, 4, 8])
+def test_spmv_accumulates_like_oracle(cuda, tag, dt, r):
+    """y += A x on a nonzero y, repeated 16 times like the reference driver
+    (load_mm_and_compare.cpp:505-507): bit-identical to the oracle."""
+    f = oracle.beta_spmv_f64 if dt == np.float64 else oracle.beta_spmv_f32
+    for csr in irregular_cases():
+        vals = csr.values.astype(dt)
+        brptr, headers, ov = oracle.csr_to_beta(r, csr.rowptr, csr.colidx, vals)
+        m = converted(csr, dt, r)
+        gb, gh, gv = m.arrays()
+        assert np.array_equal(gb, brptr) and np.array_equal(gh, headers) and gv.tobytes() == ov.tobytes()
+        x = M.x_vector(csr.ncols, 3, dt)
+        y0 = M.x_vector(csr.nrows, 4, dt)
+        yo = y0.copy()
+        for _ in range(16):
+            f(r, csr.nrows, brptr, headers, ov, x, yo)
+        y = dev(y0)
+        xd = dev(x)
+        for _ in range(16):
+            S.SPC5_Spmv(m, xd, y)
+        torch.cuda.synchronize()
+        assert y.cpu().numpy().tobytes() == yo.tobytes(), csr.name
+
+
+@pytest.mark.parametrize("r", [1, 2, 4, 8])
+def test_mixed_precision(cuda, r):
+    for csr in list(irregular_cases())[:5]:
+        m = converted(csr, np.float32, r)
+        brptr, headers, v32 = m.arrays()
+        x = M.x_vector(csr.ncols, 5)
+        x32 = x.astype(np.float32)
+        y = torch.zeros(csr.nrows, dtype=torch.float64, device="cuda")
+        S.SPC5_Spmv_mixed(m, dev(x32), y)
+        torch.cuda.synchronize()
+        y = y.cpu().numpy()
+        yo = oracle.beta_spmv_mixed(r, csr.nrows, brptr, headers, v32, x32, np.zeros(csr.nrows))
+        assert y.tobytes() == yo.tobytes(), csr.name
+        y64, absrow = oracle.csr_spmv_f64(csr.rowptr, csr.colidx, csr.values, x, np.zeros(csr.nrows))
+        if csr.nnz:
+            assert np.abs(y - y64).max() / np.abs(y64).max() <= 1e-6
+            assert (np.abs(y - y64) / np.maximum(absrow, 1e-300)).max() <= 2.5e-7
+
+
+def test_fp64_matches_csr_oracle_componentwise(cuda):
+    csr = M.powerlaw(50000, seed=2)
+    x = M.x_vector(csr.ncols, 6)
+    y64, absrow = oracle.csr_spmv_f64(csr.rowptr, csr.colidx, csr.values, x, np.zeros(csr.nrows))
+    for r in (1, 2, 4, 8):
+        y = gpu_spmv(converted(csr, np.float64, r), x, np.zeros(csr.nrows))
+        assert (np.abs(y - y64) / np.maximum(absrow, 1e-300)).max() <= 1e-13
+
+
+def test_errors_are_status_codes(cuda):
+    bad = M.CSR(2, 4, np.array([0, 2, 3], np.int32), np.array([3, 1, 0], np.int32), np.ones(3), "unsorted")
+    with pytest.raises(S.SPC5Error) as e:
+        S.csr_matrix(bad.rowptr, bad.colidx, bad.values, bad.ncols)
+    assert e.value.status == 1
+    out_of_range = M.CSR(1, 2, np.array([0, 1], np.int32), np.array([5], np.int32), np.ones(1), "oor")
+    with pytest.raises(S.SPC5Error):
+        S.csr_matrix(out_of_range.rowptr, out_of_range.colidx, out_of_range.values, out_of_range.ncols)
+    a = M.poisson2d(8)
+    m = S.csr_matrix(a.rowptr, a.colidx, a.values, a.ncols)
+    with pytest.raises(S.SPC5Error) as e:
+        S.CSR_to_SPC5(m, 9)
+    assert e.value.status == 4
+    with pytest.raises(S.SPC5Error):
+        S.SPC5_Spmv(m, torch.zeros(64, dtype=torch.float64, device="cuda"),
+                    torch.zeros(64, dtype=torch.float64, device="cuda"))
+    S.CSR_to_SPC5(m, S.FORMAT_2rVc)
+    with pytest.raises(S.SPC5Error):
+        S.CSR_to_SPC5(m, S.FORMAT_4rVc)  # already converted
+    with pytest.raises(S.SPC5Error):
+        S.SPC5_Spmv_mixed(m, torch.zeros(64, dtype=torch.float32, device="cuda"),
+                          torch.zeros(64, dtype=torch.float64, device="cuda"))
+    with pytest.raises(S.SPC5Error):
+        S.core_spmv(3, 64, *[torch.zeros(1, dtype=t, device="cuda") for t in
+                             (torch.int32, torch.uint8, torch.float64, torch.float64, torch.float64)])
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("which", ["powerlaw", "stencil27"])
+def test_full_size_bit_exact(cuda, which):
+    """The full-size workloads: device conversion byte-identical and FP64 SpMV
+    bit-identical to the oracle, for every r."""
+    csr = M.powerlaw() if which == "powerlaw" else M.stencil27(160)
+    x = M.x_vector(csr.ncols, 0)
+    rs = (1, 2, 4, 8) if which == "powerlaw" else (4,)
+    for r in rs:
+        brptr, headers, ov = oracle.csr_to_beta(r, csr.rowptr, csr.colidx, csr.values)
+        m = converted(csr, np.float64, r)
+        gb, gh, gv = m.arrays()
+        assert np.array_equal(gb, brptr) and np.array_equal(gh, headers) and gv.tobytes() == ov.tobytes()
+        yo = oracle.beta_spmv_f64(r, csr.nrows, brptr, headers, ov, x, np.zeros(csr.nrows))
+        y = gpu_spmv(m, x, np.zeros(csr.nrows))
+        assert y.tobytes() == yo.tobytes()
+        del m
