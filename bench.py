@@ -65,20 +65,21 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def build_workload(name):
+def build_workload(name, size=None):
     if name == "powerlaw":
-        return M.powerlaw()
+        return M.powerlaw(size or 4_000_000)
     if name == "stencil27":
-        return M.stencil27(160)
+        return M.stencil27(size or 160)
     if name == "poisson":
         return M.poisson2d(512)
     raise ValueError(name)
 
 
 def workload_desc(name, csr):
-    return {"powerlaw": "power-law N=4,000,000 Zipf(1.8)+3 clipped to 2000, 70% runs U[1,16] near "
+    return {"powerlaw": f"power-law N={csr.nrows:,} Zipf(1.8)+3 clipped to 2000, 70% runs U[1,16] near "
                         "diagonal (sigma N/100), U[-1,1] values, seed 1",
-            "stencil27": "27-point stencil 160^3, diag 26, neighbours -1+U[-1e-3,1e-3], seed 2",
+            "stencil27": f"27-point stencil {round(csr.nrows ** (1 / 3))}^3, diag 26, neighbours "
+                         "-1+U[-1e-3,1e-3], seed 2",
             "poisson": "5-point Poisson 512^2, diag 4, off -1"}[name] + f"; nnz={csr.nnz}"
 
 
@@ -184,7 +185,7 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "host CPU has no AVX-512 (reference build "
                                                                "uses USE_AVX512 kernels)"}))
         return 0
-    csr = build_workload(args.workload)
+    csr = build_workload(args.workload, args.size)
     threads = oracle.ref().ref_max_threads()
     xp = oracle.x_padded(M.x_vector(csr.ncols, 0))
     mats, step_bytes = [], 0
@@ -210,8 +211,8 @@ def run_reference(args):
             "config": {"workload": args.workload, "desc": workload_desc(args.workload, csr),
                        "formats": list(FORMATS), "l2": "inputs larger than L2"},
             "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": "reference",
-                             "sample": f"{args.steps} steps x 4 SPC5_Spmv_omp calls (r=1,2,4,8) on the full "
-                                       f"matrix, OMP threads={threads}"},
+                             "sample": f"{args.steps} steps x {len(FORMATS)} SPC5_Spmv_omp calls (r={FORMATS}) on the "
+                                       f"full matrix, OMP threads={threads}"},
             "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -247,7 +248,7 @@ def run_gpu(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    csr = build_workload(args.workload)
+    csr = build_workload(args.workload, args.size)
     stream = torch.cuda.current_stream()
     mats, bytes_of = [], {}
     for r in FORMATS:
@@ -356,11 +357,11 @@ def run_gpu(args):
     if rank == 0:
         cpu = None
         if not args.no_cpu_baseline:
-            res = cpu_baseline(csr)
+            res = cpu_baseline(csr, formats=FORMATS)
             if res is not None:
                 gbs, threads, nsteps, secs = res
                 cpu = {"value": round(gbs, 3), "unit": UNIT, "cores": threads, "kind": "reference",
-                       "sample": f"{nsteps} steps x 4 SPC5_Spmv_omp (r=1,2,4,8) on the full matrix, "
+                       "sample": f"{nsteps} steps x {len(formats)} SPC5_Spmv_omp (r={formats}) on the full matrix, "
                                  f"{secs:.1f} s"}
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
@@ -370,7 +371,7 @@ def run_gpu(args):
             "config": {"workload": args.workload, "desc": workload_desc(args.workload, csr),
                        "formats": list(FORMATS), "nrows": csr.nrows, "nnz": csr.nnz,
                        "blocks": {str(r): m.numberOfBlocks for r, m in mats},
-                       "l2": "inputs larger than L2 (4 matrices of >0.5 GB read in turn)",
+                       "l2": "inputs larger than L2 (every matrix > 126 MB, read in turn)",
                        "parallelism": f"replica per GPU x{world}"},
             "per_format_gbs": {str(r): round(bytes_of[r] / (per_r_ms[r] * 1e-3) / 1e9, 2) for r in FORMATS},
             "gflops": round(2 * csr.nnz * len(FORMATS) * args.steps * world / (ms * 1e-3) / 1e9, 2),
@@ -400,6 +401,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["powerlaw", "stencil27", "poisson"], default="powerlaw")
+    ap.add_argument("--size", type=int, default=None,
+                    help="smaller workload for profiling (rows for powerlaw, grid edge for stencil27)")
+    ap.add_argument("--formats", default="1,2,4,8", help="comma list of r to run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--traffic", type=float, default=None,
@@ -407,6 +411,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    global FORMATS
+    FORMATS = tuple(int(t) for t in args.formats.split(","))
     if args.impl == "reference":
         return run_reference(args)
     return run_gpu(args)

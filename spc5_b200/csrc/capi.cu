@@ -131,6 +131,8 @@ struct spc5cuda_mat {
     Owned brptr;    // rowsSize after conversion: ceil(nrows/r)+1 block offsets
     Owned headers;  // blocksColumnIndexesWithMasks
     Owned valptr;   // ceil(nrows/r)+1 value offsets (not in the reference format)
+    Owned gstart;   // ngroups+1 block-row starts of the per-group ranges
+    int ngroups = 0;
 
     int nbr() const { return r ? div_up(nrows, r) : 0; }
     BetaView view() const {
@@ -142,11 +144,19 @@ struct spc5cuda_mat {
         v.headers = headers.as<uint8_t>();
         v.values = values.p;
         v.valptr = valptr.as<int>();
+        v.gstart = gstart.as<int>();
+        v.ngroups = ngroups;
         return v;
     }
     long device_bytes() const {
         return long(rowptr.bytes + colidx.bytes + values.bytes + brptr.bytes + headers.bytes +
-                    valptr.bytes);
+                    valptr.bytes + gstart.bytes);
+    }
+    // The per-group block-row ranges for the current device.
+    void build_partition(cudaStream_t s) {
+        ngroups = spmv_groups(vs_of(value_type), r);
+        gstart.alloc(sizeof(int) * size_t(ngroups + 1));
+        launch_partition(nbr(), brptr.as<int>(), ngroups, gstart.as<int>(), s);
     }
 };
 
@@ -197,12 +207,16 @@ void core_spmv(int r, long nbRows, const int* rowsSizes, const unsigned char* he
     require(r == 1 || r == 2 || r == 4 || r == 8, SPC5CUDA_ERR_FORMAT, "r must be 1, 2, 4 or 8");
     require(nbRows >= 0 && nbRows < (1L << 31), SPC5CUDA_ERR_INVALID, "nbRows out of range");
     if (nbRows == 0) return;
-    require(rowsSizes && headers && values && x && y, SPC5CUDA_ERR_INVALID, "null pointer");
-    require(aligned(headers, 4) && aligned(values, sizeof(T)), SPC5CUDA_ERR_INVALID,
-            "misaligned array");
+    // headers / values may be null only for a matrix without blocks
+    require(rowsSizes && x && y, SPC5CUDA_ERR_INVALID, "null pointer");
+    require(aligned(headers, 4) && aligned(values, 16) && aligned(rowsSizes, 4),
+            SPC5CUDA_ERR_INVALID, "misaligned array (headers 4 bytes, values 16 bytes)");
     const int nbr = div_up(nbRows, r);
+    const int ngroups = spmv_groups(sizeof(T) == 8 ? 8 : 16, r);
     DevBuf valptr(sizeof(int) * size_t(nbr + 1), s);
+    DevBuf gstart(sizeof(int) * size_t(ngroups + 1), s);
     valptr_from_headers(sizeof(T) == 8 ? 1 : 2, r, nbr, rowsSizes, headers, valptr.as<int>(), s);
+    launch_partition(nbr, rowsSizes, ngroups, gstart.as<int>(), s);
     BetaView v;
     v.r = r;
     v.nrows = int(nbRows);
@@ -211,6 +225,8 @@ void core_spmv(int r, long nbRows, const int* rowsSizes, const unsigned char* he
     v.headers = headers;
     v.values = values;
     v.valptr = valptr.as<int>();
+    v.gstart = gstart.as<int>();
+    v.ngroups = ngroups;
     if constexpr (sizeof(T) == 8)
         launch_spmv_f64(v, x, y, s);
     else
@@ -344,6 +360,7 @@ spc5cuda_status spc5cuda_mat_create_beta(spc5cuda_mat** out, int value_type, int
             } else {
                 SPC5_CUDA(cudaMemsetAsync(m->valptr.p, 0, sizeof(int), s));
             }
+            m->build_partition(s);
             SPC5_CUDA(cudaStreamSynchronize(s));
         } catch (...) {
             delete m;
@@ -419,6 +436,8 @@ spc5cuda_status spc5cuda_convert(spc5cuda_mat* m, int format, void* stream) {
         m->r = r;
         m->format = format;
         m->nblocks = nb;
+        m->build_partition(s);
+        SPC5_CUDA(cudaStreamSynchronize(s));
     });
 }
 

@@ -83,7 +83,8 @@ __device__ __forceinline__ int load_header(const uint8_t* __restrict__ hdr, long
         return int(lw[0]);
     } else {
         const unsigned sh = unsigned(off & 3) * 8u;
-        mw[0] = __funnelshift_r(lw[1], lw[2], sh);
+        // the record ends inside this word: clear the next record's bytes
+        mw[0] = __funnelshift_r(lw[1], lw[2], sh) & ((1u << (8 * H::MASK_BYTES_TOTAL)) - 1u);
         return int(__funnelshift_r(lw[0], lw[1], sh));
     }
 }

@@ -45,7 +45,16 @@ struct BetaView {
     const uint8_t* headers;
     const void* values;
     const int* valptr;  // nbr + 1 value offsets
+    const int* gstart;  // ngroups + 1 block-row starts of the group ranges
+    int ngroups;
 };
+
+// Number of VS-lane groups the SpMV kernels launch on the current device
+// for rows-per-block r: one wave of resident CTAs.
+int spmv_groups(int vs, int r);
+
+// gstart[0..ngroups] = block-row ranges holding ~nblocks/ngroups blocks each.
+void launch_partition(int nbr, const int* brptr, int ngroups, int* gstart, cudaStream_t s);
 
 void launch_spmv_f64(const BetaView& m, const double* x, double* y, cudaStream_t s);
 void launch_spmv_f32(const BetaView& m, const float* x, float* y, cudaStream_t s);
