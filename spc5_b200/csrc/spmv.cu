@@ -115,34 +115,40 @@ __device__ __forceinline__ uint32_t lanes_of(const uint32_t (&mw)[Header<LT, R>:
     }
 }
 
-// Kernel geometry per layout.
-template <class LT, class V, class X>
+// Geometry of the kernel: a group of VS lanes (lane c = column c of every
+// block) owns one block-row stream; GPW groups per warp run in lockstep.
+template <class LT, int R, class V, class X, class A>
 struct Geo {
     static constexpr int VS = Layout<LT>::VS;
     static constexpr int THREADS = 128;
-    static constexpr int GPC = THREADS / VS;                // groups per CTA
+    static constexpr int GPW = 32 / VS;                      // groups per warp
+    static constexpr int GPC = THREADS / VS;                 // groups per CTA
     static constexpr int EPU = 16 / int(sizeof(V));          // values per 16-byte unit
     static constexpr int CAP = 1024 / int(sizeof(V));        // staged values per window
     static constexpr int VBUF = CAP + 2 * EPU;               // + alignment slack
     static constexpr int VBYTES = VBUF * int(sizeof(V));
     static constexpr int XBYTES = VS * VS * int(sizeof(X));  // x of one window: [block][column]
-    static constexpr int BUF_BYTES = ((VBYTES + XBYTES) + 15) / 16 * 16;
-    static constexpr int GROUP_BYTES = 2 * BUF_BYTES;        // double buffered
+    static constexpr int BUF_BYTES = (VBYTES + XBYTES + 15) / 16 * 16;
+    static constexpr int RED_BYTES = R > 1 ? (R * VS * int(sizeof(A)) + 15) / 16 * 16 : 0;
+    static constexpr int GROUP_BYTES = 2 * BUF_BYTES + RED_BYTES;  // double-buffered windows
     static constexpr int SMEM = GPC * GROUP_BYTES;
+    static constexpr int MW = Header<LT, R>::MASK_WORDS;
+    static constexpr int PW = (R + 3) / 4;                   // packed sub-row prefixes
+    static_assert(CAP >= VS * R, "a block must fit one window");
 };
 
-// One window of a group: lane j describes block j (j < n).
+// One window of a group: lane j describes block j of the window (j < n).
 template <class LT, int R>
 struct Win {
     static constexpr int MW = Header<LT, R>::MASK_WORDS;
-    static constexpr int PW = (R + 3) / 4;  // packed per-sub-row value prefixes (bytes)
+    static constexpr int PW = (R + 3) / 4;
     uint32_t mw[MW];
-    uint32_t pre[PW];
-    int voff;  // offset of the block's first value in the staging buffer
-    int n;     // blocks in the window (group-uniform)
+    uint32_t pre[PW];  // exclusive prefix of the sub-row value counts, one byte per sub-row
+    int voff;          // staging-buffer index of the block's first value
+    int n;             // blocks in the window (group-uniform)
 };
 
-// Raw headers of up to VS blocks starting at block p: lane j holds block p + j.
+// Headers of up to VS blocks starting at block p: lane j holds block p + j.
 template <class LT, int R>
 struct Raw {
     uint32_t mw[Header<LT, R>::MASK_WORDS];
@@ -151,13 +157,13 @@ struct Raw {
 };
 
 template <class LT, int R>
-__device__ __forceinline__ void load_raw(Raw<LT, R>& rw, const uint8_t* __restrict__ headers, long p,
-                                         long b_stop, int c) {
-    rw.ok = p + c < b_stop;
+__device__ __forceinline__ void load_raw(Raw<LT, R>& rw, const uint8_t* __restrict__ headers, int p,
+                                         int b_stop, int j) {
+    rw.ok = p + j < b_stop;
     rw.col = 0;
 #pragma unroll
     for (int q = 0; q < Header<LT, R>::MASK_WORDS; ++q) rw.mw[q] = 0u;
-    if (rw.ok) rw.col = load_header_stream<LT, R>(headers, p + c, rw.mw);
+    if (rw.ok) rw.col = load_header_stream<LT, R>(headers, long(p + j), rw.mw);
 }
 
 template <class LT, int R, class V, class X, class A, class Y>
@@ -166,24 +172,24 @@ __global__ void __launch_bounds__(128)
            const V* __restrict__ values, const int* __restrict__ valptr,
            const int* __restrict__ gstart, int ngroups, const X* __restrict__ x,
            Y* __restrict__ y) {
-    using G = Geo<LT, V, X>;
-    constexpr int VS = G::VS;
-    constexpr int MW = Header<LT, R>::MASK_WORDS;
-    constexpr int PW = Win<LT, R>::PW;
+    using G = Geo<LT, R, V, X, A>;
+    constexpr int VS = G::VS, MW = G::MW, PW = G::PW;
     constexpr int MB = Layout<LT>::MASK_BYTES;
+    constexpr bool Y_ATOMIC = sizeof(Y) == 8;  // red.add.f64 is y + s rounded once
     constexpr unsigned FULL = 0xffffffffu;
+    constexpr unsigned VSMASK = (VS == 32) ? FULL : ((1u << VS) - 1u);
     extern __shared__ __align__(16) unsigned char smem[];
 
     const int lane = threadIdx.x & 31;
     const int c = lane & (VS - 1);
     const int gbase_lane = lane & ~(VS - 1);
     const uint32_t below = (1u << c) - 1u;
-    const int gl = threadIdx.x / VS;
-    const int group = blockIdx.x * G::GPC + gl;
-    const uint32_t sgroup = uint32_t(__cvta_generic_to_shared(smem)) + uint32_t(gl * G::GROUP_BYTES);
-    unsigned char* pgroup = smem + gl * G::GROUP_BYTES;
+    const int gi = threadIdx.x / VS;
+    const int group = blockIdx.x * G::GPC + gi;
+    const uint32_t sgroup = uint32_t(__cvta_generic_to_shared(smem)) + uint32_t(gi * G::GROUP_BYTES);
+    unsigned char* pgroup = smem + gi * G::GROUP_BYTES;
+    A* red = reinterpret_cast<A*>(pgroup + 2 * G::BUF_BYTES);
 
-    // this group's block-row range; groups past ngroups get an empty range
     int r_begin = 0, r_end = 0;
     if (group < ngroups) {
         r_begin = __ldg(gstart + group);
@@ -191,9 +197,9 @@ __global__ void __launch_bounds__(128)
     }
     if (!__any_sync(FULL, r_begin < r_end)) return;
     const bool has = r_begin < r_end;
-    long b_stop = has ? __ldg(brptr + r_end) : 0;
-    long p = has ? __ldg(brptr + r_begin) : 0;   // first block of the next window to stage
-    long v_next = has ? __ldg(valptr + r_begin) : 0;
+    const int b_stop = has ? __ldg(brptr + r_end) : 0;
+    int p = has ? __ldg(brptr + r_begin) : 0;  // first block of the next window to stage
+    int v_next = has ? __ldg(valptr + r_begin) : 0;
 
     // row bookkeeping: current block-row row = rbase + k, rend = its end block
     int row = r_begin, rbase = r_begin, k = 0;
@@ -201,32 +207,50 @@ __global__ void __launch_bounds__(128)
     int ends_nxt = (has && rbase + 1 + VS + c <= r_end) ? __ldg(brptr + rbase + 1 + VS + c) : 0x7fffffff;
     int rend = __shfl_sync(FULL, ends, 0, VS);
     Y ycur = Y(0);
-    if (has && c < R && long(row) * R + c < nrows) ycur = y[long(row) * R + c];
+    if (!Y_ATOMIC && has && c < R && row * R + c < nrows) ycur = y[row * R + c];
 
     A acc[R];
 #pragma unroll
     for (int i = 0; i < R; ++i) acc[i] = A(0);
 
-    // Flush every group whose current block-row ends at block position `pos`
-    // (need), repeating for empty block-rows; warp-uniform control flow.
-    auto flush_while = [&](bool active, long pos) {
+    // Flush every group whose current block-row ends at block position pos,
+    // repeating for empty block-rows; warp-uniform control flow.  The row sum
+    // is the _mm512_reduce_add tree over the VS lane accumulators: distance
+    // VS/2 first, then VS/4, ..., 1.
+    auto flush_while = [&](bool active, int pos) {
         for (;;) {
-            const bool need = active && row < r_end && pos == long(rend);
+            const bool need = active && row < r_end && pos == rend;
             if (!__any_sync(FULL, need)) break;
-            A t[R];
+            A s = A(0);
+            if constexpr (R == 1) {
+                s = acc[0];
 #pragma unroll
-            for (int i = 0; i < R; ++i) {
-                t[i] = acc[i];
+                for (int d = VS / 2; d >= 1; d >>= 1) s += __shfl_xor_sync(FULL, s, d, VS);
+            } else {
+                if (need) {
 #pragma unroll
-                for (int d = VS / 2; d >= 1; d >>= 1) t[i] += __shfl_xor_sync(FULL, t[i], d, VS);
+                    for (int i = 0; i < R; ++i) red[i * VS + c] = acc[i];
+                }
+                __syncwarp();
+                if (need && c < R) {
+                    A a[VS];
+#pragma unroll
+                    for (int e = 0; e < VS; ++e) a[e] = red[c * VS + e];
+#pragma unroll
+                    for (int d = VS / 2; d >= 1; d >>= 1) {
+#pragma unroll
+                        for (int e = 0; e < d; ++e) a[e] = a[e] + a[e + d];
+                    }
+                    s = a[0];
+                }
+                __syncwarp();
             }
-            A s = t[0];
-#pragma unroll
-            for (int i = 1; i < R; ++i)
-                if (c == i) s = t[i];
             if (need) {
-                const long yrow = long(row) * R + c;
-                if (c < R && yrow < nrows) y[yrow] = ycur + Y(s);
+                const int yrow = row * R + c;
+                if (c < R && yrow < nrows) {
+                    if constexpr (Y_ATOMIC) atomicAdd(y + yrow, Y(s));
+                    else y[yrow] = ycur + Y(s);
+                }
 #pragma unroll
                 for (int i = 0; i < R; ++i) acc[i] = A(0);
                 ++row;
@@ -236,14 +260,16 @@ __global__ void __launch_bounds__(128)
                     ends = ends_nxt;
                     ends_nxt = (rbase + 1 + VS + c <= r_end) ? __ldg(brptr + rbase + 1 + VS + c) : 0x7fffffff;
                 }
-                const long ynext = long(row) * R + c;
-                if (c < R && row < r_end && ynext < nrows) ycur = y[ynext];
+                if constexpr (!Y_ATOMIC) {
+                    const int ynext = row * R + c;
+                    if (c < R && row < r_end && ynext < nrows) ycur = y[ynext];
+                }
             }
             rend = __shfl_sync(FULL, ends, k, VS);
         }
     };
 
-    // ---- stage one window: headers in rw (blocks p ...) -> win, copies into buffer `bi`
+    // ---- stage one window: headers rw (blocks p ...) -> win; values and x into buffer bi
     auto stage = [&](const Raw<LT, R>& rw, Win<LT, R>& win, int bi) {
         int tot = 0;
 #pragma unroll
@@ -255,17 +281,14 @@ __global__ void __launch_bounds__(128)
             const int t = __shfl_up_sync(FULL, incl, d, VS);
             if (c >= d) incl += t;
         }
-        const unsigned fit = (__ballot_sync(FULL, rw.ok && incl <= G::CAP) >> gbase_lane) &
-                             ((VS == 32) ? FULL : ((1u << VS) - 1u));
-        const int n = __popc(fit);
+        const int n = __popc((__ballot_sync(FULL, rw.ok && incl <= G::CAP) >> gbase_lane) & VSMASK);
         const int tv = __shfl_sync(FULL, incl, (n > 0 ? n : 1) - 1, VS);
-        const long s0 = v_next & ~long(G::EPU - 1);
-        const int shift = int(v_next - s0);
+        const int s0 = v_next & ~(G::EPU - 1);
+        const int shift = v_next - s0;
         win.n = n;
 #pragma unroll
         for (int q = 0; q < MW; ++q) win.mw[q] = rw.mw[q];
         win.voff = shift + incl - tot;
-        // packed exclusive prefix of the sub-row value counts inside the block
         {
             uint32_t run = 0;
 #pragma unroll
@@ -279,19 +302,23 @@ __global__ void __launch_bounds__(128)
         const uint32_t vb = sgroup + uint32_t(bi * G::BUF_BYTES);
         if (n > 0) {
             const int units = (shift + tv + G::EPU - 1) / G::EPU;
-            for (int u = c; u < units; u += VS)
-                cp_async16(vb + uint32_t(u) * 16u, values + s0 + long(u) * G::EPU);
-            if (c < n) {
-                const uint32_t lor = lanes_of<LT, R>(rw.mw);
-                const uint32_t xb = vb + uint32_t(G::VBYTES) + uint32_t(c * VS) * uint32_t(sizeof(X));
+            const V* src = values + s0;
+            for (int u = c; u < units; u += VS) cp_async16(vb + uint32_t(u) * 16u, src + u * G::EPU);
+        }
+        // x: lane c copies column c of every block that holds a value there
+        {
+            const uint32_t lor = lanes_of<LT, R>(rw.mw);
+            const uint32_t xb = vb + uint32_t(G::VBYTES) + uint32_t(c) * uint32_t(sizeof(X));
 #pragma unroll
-                for (int t = 0; t < VS; ++t)
-                    if ((lor >> t) & 1u)
-                        cp_async_small<int(sizeof(X))>(xb + uint32_t(t) * uint32_t(sizeof(X)), x + rw.col + t);
+            for (int j = 0; j < VS; ++j) {
+                const int cj = __shfl_sync(FULL, rw.col, j, VS);
+                const uint32_t lj = __shfl_sync(FULL, lor, j, VS);
+                if (j < n && ((lj >> c) & 1u))
+                    cp_async_small<int(sizeof(X))>(xb + uint32_t(j * VS) * uint32_t(sizeof(X)), x + (cj + c));
             }
         }
         cp_async_commit();
-        v_next += tv * (n > 0);
+        v_next += (n > 0) ? tv : 0;
         p += n;
     };
 
@@ -299,17 +326,33 @@ __global__ void __launch_bounds__(128)
     Raw<LT, R> raw;
     load_raw<LT, R>(raw, headers, p, b_stop, c);
     Win<LT, R> cur;
-    long wstart = p;  // first block of the current window
+    int wstart = p;  // first block of the current window
     stage(raw, cur, 0);
     load_raw<LT, R>(raw, headers, p, b_stop, c);
     int bi = 0;
 
     while (__any_sync(FULL, cur.n > 0)) {
-        // stage window w+1 into the other buffer, load headers of window w+2
         Win<LT, R> nxt;
-        const long nstart = p;
+        const int nstart = p;
         stage(raw, nxt, bi ^ 1);
         load_raw<LT, R>(raw, headers, p, b_stop, c);
+
+        // block positions of this window where a block-row of some group ends
+        // (known row ends: ends of rows rbase+1 .. rbase+VS, ends_nxt beyond);
+        // positions past the last known end are checked individually.
+        uint32_t rmask;
+        {
+            const int rel = ends - wstart;
+            uint32_t mine = (rel >= 0 && rel < VS) ? (1u << rel) : 0u;
+            const int last = __shfl_sync(FULL, ends_nxt, VS - 1, VS);
+            const int lrel = last - wstart;
+            if (c == 0 && lrel < VS) mine |= VSMASK << (lrel < 0 ? 0 : lrel);
+            const int rel2 = ends_nxt - wstart;
+            if (rel2 >= 0 && rel2 < VS) mine |= 1u << rel2;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) mine |= __shfl_xor_sync(FULL, mine, d);
+            rmask = mine;
+        }
         cp_async_wait_prev();
         __syncwarp();
 
@@ -317,6 +360,7 @@ __global__ void __launch_bounds__(128)
         const X* xbuf = reinterpret_cast<const X*>(pgroup + bi * G::BUF_BYTES + G::VBYTES);
 #pragma unroll
         for (int j = 0; j < VS; ++j) {
+            if (!__any_sync(FULL, j < cur.n)) break;
             const bool act = j < cur.n;
             uint32_t bm[MW];
 #pragma unroll
@@ -325,22 +369,18 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
             for (int q = 0; q < PW; ++q) bp[q] = __shfl_sync(FULL, cur.pre[q], j, VS);
             const int voff = __shfl_sync(FULL, cur.voff, j, VS);
-            flush_while(act, wstart + j);
+            if ((rmask >> j) & 1u) flush_while(act, wstart + j);
             if (act) {
                 const A xv = A(xbuf[j * VS + c]);
                 if constexpr (MB == 1 && R >= 2) {
-                    // byte-parallel ranks of lane c in every sub-row mask
 #pragma unroll
                     for (int q = 0; q < MW; ++q) {
-                        const uint32_t rk = popc_bytes(bm[q] & (below * 0x01010101u));
-                        const uint32_t Q = bp[q] + rk;
+                        const uint32_t Q = bp[q] + popc_bytes(bm[q] & (below * 0x01010101u));
 #pragma unroll
                         for (int ii = 0; ii < 4; ++ii) {
                             const int i = q * 4 + ii;
-                            if (i < R && ((bm[q] >> (ii * 8 + c)) & 1u)) {
-                                const int idx = voff + int((Q >> (ii * 8)) & 0xFFu);
-                                acc[i] = fma(A(vbuf[idx]), xv, acc[i]);
-                            }
+                            if (i < R && ((bm[q] >> (ii * 8 + c)) & 1u))
+                                acc[i] = fma(A(vbuf[voff + int((Q >> (ii * 8)) & 0xFFu)]), xv, acc[i]);
                         }
                     }
                 } else {
@@ -348,8 +388,7 @@ __global__ void __launch_bounds__(128)
                     for (int i = 0; i < R; ++i) {
                         const uint32_t m = mask_of<LT, R>(bm, i);
                         if ((m >> c) & 1u) {
-                            const int idx = voff + int((bp[i >> 2] >> ((i & 3) * 8)) & 0xFFu) +
-                                            __popc(m & below);
+                            const int idx = voff + int((bp[i >> 2] >> ((i & 3) * 8)) & 0xFFu) + __popc(m & below);
                             acc[i] = fma(A(vbuf[idx]), xv, acc[i]);
                         }
                     }
@@ -366,8 +405,7 @@ __global__ void __launch_bounds__(128)
     for (;;) {
         const bool need = row < r_end;
         if (!__any_sync(FULL, need)) break;
-        const long pos = need ? long(rend) : -1;
-        flush_while(need, pos);
+        flush_while(need, need ? rend : -1);
     }
 }
 
@@ -399,11 +437,11 @@ void set_smem(K kernel, int bytes) {
 template <class LT, class V, class X, class A, class Y>
 void launch_impl(const BetaView& m, const X* x, Y* y, cudaStream_t s) {
     if (m.nbr <= 0) return;
-    using G = Geo<LT, V, X>;
     const V* vals = static_cast<const V*>(m.values);
-    const int ctas = (m.ngroups + G::GPC - 1) / G::GPC;
 #define SPC5_LAUNCH(R_)                                                                          \
     {                                                                                            \
+        using G = Geo<LT, R_, V, X, A>;                                                          \
+        const int ctas = (m.ngroups + G::GPC - 1) / G::GPC;                                      \
         auto kern = k_spmv<LT, R_, V, X, A, Y>;                                                  \
         set_smem(kern, G::SMEM);                                                                 \
         kern<<<ctas, G::THREADS, G::SMEM, s>>>(m.nrows, m.brptr, m.headers, vals, m.valptr,      \
@@ -426,10 +464,10 @@ namespace {
 
 template <class LT, class V, class X, class A, class Y>
 int occupancy(int r) {
-    using G = Geo<LT, V, X>;
     int n = 0;
 #define SPC5_OCC(R_)                                                                             \
     {                                                                                            \
+        using G = Geo<LT, R_, V, X, A>;                                                          \
         auto kern = k_spmv<LT, R_, V, X, A, Y>;                                                  \
         set_smem(kern, G::SMEM);                                                                 \
         SPC5_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, G::THREADS, G::SMEM)); \
@@ -447,16 +485,25 @@ int occupancy(int r) {
 
 }  // namespace
 
+namespace {
+
+template <class LT, class V>
+int groups_per_cta(int) {
+    return Geo<LT, 1, V, V, V>::GPC;
+}
+
+}  // namespace
+
 int spmv_groups(int vs, int r) {
     // one wave of resident CTAs: the static partition then has no tail
     int per_sm, gpc;
     if (vs == 8) {
         per_sm = occupancy<double, double, double, double, double>(r);
-        gpc = Geo<double, double, double>::GPC;
+        gpc = groups_per_cta<double, double>(r);
     } else {
         per_sm = std::min(occupancy<float, float, float, float, float>(r),
                           occupancy<float, float, float, double, double>(r));
-        gpc = Geo<float, float, float>::GPC;
+        gpc = groups_per_cta<float, float>(r);
     }
     per_sm = std::max(1, std::min(per_sm, SPMV_CTAS_PER_SM));
     return sm_count() * per_sm * gpc;
