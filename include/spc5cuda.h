@@ -182,6 +182,61 @@ SPC5CUDA_API spc5cuda_status spc5cuda_spmv(const spc5cuda_mat* mat, const void* 
 SPC5CUDA_API spc5cuda_status spc5cuda_spmv_mixed(const spc5cuda_mat* mat, const float* x, double* y,
                                     void* stream);
 
+/* Multi-RHS SpMM (no counterpart in the reference): Y += A X for k
+ * right-hand sides.  X is row-major ncols x k with leading dimension
+ * ldx >= k (the k values of one matrix column are contiguous), Y row-major
+ * nrows x k with ldy >= k.  Column j of Y is bit-identical to spc5cuda_spmv
+ * with column j of X.  k <= 16 runs in one pass over the matrix for r <= 2
+ * (8 for r = 4, 4 for r = 8); larger k runs several passes. */
+SPC5CUDA_API spc5cuda_status spc5cuda_spmm(const spc5cuda_mat* mat, int k, const void* X,
+                                           long ldx, void* Y, long ldy, void* stream);
+SPC5CUDA_API spc5cuda_status spc5cuda_spmm_mixed(const spc5cuda_mat* mat, int k, const float* X,
+                                                 long ldx, double* Y, long ldy, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Format selection.
+ * ---------------------------------------------------------------------- */
+
+/* SPC5_find_best (spc5.hpp:1151-1223): the reference's cubic model in the
+ * average values per block, evaluated for r = 1, 2, 4 on block counts taken
+ * on the device.  CSR handles only.  Writes r (0 if no estimate is > 0). */
+SPC5CUDA_API spc5cuda_status spc5cuda_find_best(const spc5cuda_mat* mat, int* r,
+                                                double* estimate, void* stream);
+
+#define SPC5CUDA_TUNE_MODEL 0   /* B200 cost model on device block counts   */
+#define SPC5CUDA_TUNE_MEASURE 1 /* trial conversion + timed SpMV per r      */
+
+typedef struct spc5cuda_tune {
+    int r;            /* chosen rows per block                             */
+    int pad;
+    long blocks[4];   /* block counts for r = 1, 2, 4, 8                   */
+    double est_us[4]; /* modelled or measured SpMV microseconds per r      */
+} spc5cuda_tune;
+
+/* The project's autotuner (replaces SPC5_find_best on this hardware):
+ * picks r in {1, 2, 4, 8} for a CSR handle. */
+SPC5CUDA_API spc5cuda_status spc5cuda_autotune(const spc5cuda_mat* mat, int mode,
+                                               spc5cuda_tune* out, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Batched launch (no counterpart in the reference): n converted matrices of
+ * one value type, k[i] right-hand sides each, row-major device blocks X[i]
+ * (ncols_i x k[i], ldx[i]) and Y[i] (nrows_i x k[i], ldy[i]), Y[i] += A_i X[i].
+ * create() builds the job tables and captures one CUDA graph (synchronises
+ * stream); launch() replays it on stream.  The X / Y pointers are fixed at
+ * creation.  Results per column equal spc5cuda_spmv bit for bit.
+ * ---------------------------------------------------------------------- */
+typedef struct spc5cuda_batch spc5cuda_batch;
+SPC5CUDA_API spc5cuda_status spc5cuda_batch_create(spc5cuda_batch** out, int n,
+                                                   spc5cuda_mat* const* mats, const int* k,
+                                                   void* const* X, const long* ldx,
+                                                   void* const* Y, const long* ldy, int mixed,
+                                                   void* stream);
+SPC5CUDA_API spc5cuda_status spc5cuda_batch_launch(spc5cuda_batch* batch, void* stream);
+SPC5CUDA_API spc5cuda_status spc5cuda_batch_info(const spc5cuda_batch* batch, int* nclasses,
+                                                 long* njobs);
+SPC5CUDA_API spc5cuda_status spc5cuda_batch_destroy(spc5cuda_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

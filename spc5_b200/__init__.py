@@ -43,8 +43,13 @@ EXPORTED_SYMBOLS = [
     "spc5cuda_core_spmv_f64", "spc5cuda_core_spmv_f32",
     "spc5cuda_mat_create_csr", "spc5cuda_mat_create_beta", "spc5cuda_mat_destroy",
     "spc5cuda_mat_info", "spc5cuda_block_count", "spc5cuda_convert", "spc5cuda_get_arrays",
-    "spc5cuda_spmv", "spc5cuda_spmv_mixed",
+    "spc5cuda_spmv", "spc5cuda_spmv_mixed", "spc5cuda_spmm", "spc5cuda_spmm_mixed",
+    "spc5cuda_find_best", "spc5cuda_autotune", "spc5cuda_batch_create", "spc5cuda_batch_launch",
+    "spc5cuda_batch_info", "spc5cuda_batch_destroy",
 ]
+
+TUNE_MODEL = 0
+TUNE_MEASURE = 1
 
 
 class SPC5Error(RuntimeError):
@@ -52,6 +57,10 @@ class SPC5Error(RuntimeError):
         self.status = status
         msg = _lib().spc5cuda_status_string(status).decode() if _LIB is not None else str(status)
         super().__init__(f"{what}: {msg} (status {status})" if what else msg)
+
+
+class spc5cuda_tune(C.Structure):
+    _fields_ = [("r", C.c_int), ("pad", C.c_int), ("blocks", C.c_long * 4), ("est_us", C.c_double * 4)]
 
 
 class spc5cuda_info(C.Structure):
@@ -106,6 +115,21 @@ def _lib():
         lib.spc5cuda_spmv.argtypes = [_P, _P, _P, _P]
         lib.spc5cuda_spmv_mixed.restype = _I
         lib.spc5cuda_spmv_mixed.argtypes = [_P, _P, _P, _P]
+        for n in ("spc5cuda_spmm", "spc5cuda_spmm_mixed"):
+            getattr(lib, n).restype = _I
+            getattr(lib, n).argtypes = [_P, _I, _P, _L, _P, _L, _P]
+        lib.spc5cuda_find_best.restype = _I
+        lib.spc5cuda_find_best.argtypes = [_P, C.POINTER(_I), C.POINTER(C.c_double), _P]
+        lib.spc5cuda_autotune.restype = _I
+        lib.spc5cuda_autotune.argtypes = [_P, _I, C.POINTER(spc5cuda_tune), _P]
+        lib.spc5cuda_batch_create.restype = _I
+        lib.spc5cuda_batch_create.argtypes = [C.POINTER(_P), _I, _P, _P, _P, _P, _P, _P, _I, _P]
+        lib.spc5cuda_batch_launch.restype = _I
+        lib.spc5cuda_batch_launch.argtypes = [_P, _P]
+        lib.spc5cuda_batch_info.restype = _I
+        lib.spc5cuda_batch_info.argtypes = [_P, C.POINTER(_I), C.POINTER(_L)]
+        lib.spc5cuda_batch_destroy.restype = _I
+        lib.spc5cuda_batch_destroy.argtypes = [_P]
         _LIB = lib
     return _LIB
 
@@ -297,6 +321,101 @@ def SPC5_Spmv_mixed(mat: SPC5Mat, x, y, stream=None) -> None:
     import torch
     _check(_lib().spc5cuda_spmv_mixed(mat.handle, _dptr(x, torch.float32, "x"),
                                       _dptr(y, torch.float64, "y"), _stream(stream)), "SPC5_Spmv_mixed")
+
+
+def SPC5_Spmm(mat: SPC5Mat, X, Y, stream=None) -> None:
+    """Y += A X for k right-hand sides.  X is (ncols, k) and Y (nrows, k),
+    row-major CUDA tensors (the k values of one row contiguous); column j of Y
+    is bit-identical to SPC5_Spmv with column j of X."""
+    import torch
+    dt = torch.float64 if mat.dtype == np.float64 else torch.float32
+    if X.dim() != 2 or Y.dim() != 2 or X.shape[1] != Y.shape[1]:
+        raise ValueError("X and Y must be 2-D with the same number of columns")
+    if X.stride(1) != 1 or Y.stride(1) != 1:
+        raise ValueError("X and Y must be row-major (unit stride along k)")
+    k = X.shape[1]
+    _check(_lib().spc5cuda_spmm(mat.handle, k, C.c_void_p(_check_dev(X, dt, "X")), X.stride(0),
+                                C.c_void_p(_check_dev(Y, dt, "Y")), Y.stride(0), _stream(stream)),
+           "SPC5_Spmm")
+
+
+def SPC5_Spmm_mixed(mat: SPC5Mat, X, Y, stream=None) -> None:
+    """Y += A X with FP32 values and X, FP64 accumulation and Y (row-major)."""
+    import torch
+    if X.dim() != 2 or Y.dim() != 2 or X.shape[1] != Y.shape[1]:
+        raise ValueError("X and Y must be 2-D with the same number of columns")
+    if X.stride(1) != 1 or Y.stride(1) != 1:
+        raise ValueError("X and Y must be row-major (unit stride along k)")
+    k = X.shape[1]
+    _check(_lib().spc5cuda_spmm_mixed(mat.handle, k, C.c_void_p(_check_dev(X, torch.float32, "X")),
+                                      X.stride(0), C.c_void_p(_check_dev(Y, torch.float64, "Y")),
+                                      Y.stride(0), _stream(stream)), "SPC5_Spmm_mixed")
+
+
+def _check_dev(t, dtype, what):
+    import torch
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{what} must be a CUDA tensor")
+    if t.dtype != dtype:
+        raise TypeError(f"{what} must be {dtype}, got {t.dtype}")
+    return t.data_ptr()
+
+
+def SPC5_find_best(mat: SPC5Mat, stream=None):
+    """(r, estimate) of the reference's speed model, SPC5_find_best
+    (spc5.hpp:1151-1223), on block counts taken on the device (CSR handle)."""
+    r, est = C.c_int(0), C.c_double(0.0)
+    _check(_lib().spc5cuda_find_best(mat.handle, C.byref(r), C.byref(est), _stream(stream)),
+           "SPC5_find_best")
+    return int(r.value), float(est.value)
+
+
+def autotune(mat: SPC5Mat, mode: int = TUNE_MODEL, stream=None) -> dict:
+    """The B200 autotuner on a CSR handle: {'r', 'blocks': {r: n}, 'est_us': {r: t}}."""
+    t = spc5cuda_tune()
+    _check(_lib().spc5cuda_autotune(mat.handle, int(mode), C.byref(t), _stream(stream)), "autotune")
+    rs = (1, 2, 4, 8)
+    return {"r": int(t.r), "blocks": {r: int(t.blocks[i]) for i, r in enumerate(rs)},
+            "est_us": {r: float(t.est_us[i]) for i, r in enumerate(rs)}}
+
+
+class Batch:
+    """Many converted matrices, each with its own row-major X (ncols x k) and
+    Y (nrows x k) CUDA tensors, launched together as one CUDA graph."""
+
+    def __init__(self, mats, Xs, Ys, mixed=False, stream=None):
+        import torch
+        n = len(mats)
+        self._keep = (list(mats), list(Xs), list(Ys))
+        hm = (_P * max(1, n))(*[m.handle for m in mats])
+        ks = (_I * max(1, n))(*[int(X.shape[1]) for X in Xs])
+        xp = (_P * max(1, n))(*[X.data_ptr() for X in Xs])
+        yp = (_P * max(1, n))(*[Y.data_ptr() for Y in Ys])
+        lx = (_L * max(1, n))(*[int(X.stride(0)) for X in Xs])
+        ly = (_L * max(1, n))(*[int(Y.stride(0)) for Y in Ys])
+        for X, Y in zip(Xs, Ys):
+            if not (X.is_cuda and Y.is_cuda) or X.stride(1) != 1 or Y.stride(1) != 1:
+                raise ValueError("X and Y must be row-major CUDA tensors")
+        self._h = C.c_void_p()
+        _check(_lib().spc5cuda_batch_create(C.byref(self._h), n, C.cast(hm, _P), C.cast(ks, _P),
+                                            C.cast(xp, _P), C.cast(lx, _P), C.cast(yp, _P),
+                                            C.cast(ly, _P), 1 if mixed else 0, _stream(stream)),
+               "spc5cuda_batch_create")
+        del torch
+
+    def launch(self, stream=None):
+        _check(_lib().spc5cuda_batch_launch(self._h, _stream(stream)), "spc5cuda_batch_launch")
+
+    def info(self):
+        nc, nj = C.c_int(0), C.c_long(0)
+        _check(_lib().spc5cuda_batch_info(self._h, C.byref(nc), C.byref(nj)), "spc5cuda_batch_info")
+        return int(nc.value), int(nj.value)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _LIB is not None:
+            _LIB.spc5cuda_batch_destroy(h)
+            self._h = None
 
 
 def core_spmv(r: int, nbRows: int, rowsSizes, headers, values, x, y, stream=None) -> None:

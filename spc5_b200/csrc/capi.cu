@@ -8,8 +8,7 @@
 #include <mutex>
 #include <vector>
 
-#include "common.cuh"
-#include "kernels.h"
+#include "handle.h"
 
 namespace spc5cuda {
 
@@ -31,134 +30,10 @@ namespace {
 thread_local spc5cuda_status g_last_error = SPC5CUDA_OK;
 thread_local cudaStream_t g_stream = nullptr;
 
-// Stream-ordered device buffer (cudaMallocAsync / cudaFreeAsync).
-struct DevBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-    cudaStream_t s = nullptr;
-    DevBuf() = default;
-    DevBuf(size_t n, cudaStream_t st) : bytes(n), s(st) {
-        if (n) SPC5_CUDA(cudaMallocAsync(&p, n, st));
-    }
-    ~DevBuf() {
-        if (p) cudaFreeAsync(p, s);
-    }
-    DevBuf(const DevBuf&) = delete;
-    DevBuf& operator=(const DevBuf&) = delete;
-    template <class T>
-    T* as() const { return static_cast<T*>(p); }
-};
-
-// Persistent device buffer owned by a matrix handle.
-struct Owned {
-    void* p = nullptr;
-    size_t bytes = 0;
-    void alloc(size_t n) {
-        release();
-        if (n) SPC5_CUDA(cudaMalloc(&p, n));
-        bytes = n;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-    }
-    ~Owned() { release(); }
-    template <class T>
-    T* as() const { return static_cast<T*>(p); }
-};
-
-bool aligned(const void* p, size_t a) { return (reinterpret_cast<uintptr_t>(p) % a) == 0; }
-
-int format_to_r(int format) {
-    switch (format) {
-        case SPC5CUDA_FORMAT_1rVc_WT: return 1;
-        case SPC5CUDA_FORMAT_2rVc: return 2;
-        case SPC5CUDA_FORMAT_4rVc: return 4;
-        case SPC5CUDA_FORMAT_8rVc: return 8;
-        default: return 0;
-    }
-}
-
-int r_to_format(int r) {
-    switch (r) {
-        case 1: return SPC5CUDA_FORMAT_1rVc_WT;
-        case 2: return SPC5CUDA_FORMAT_2rVc;
-        case 4: return SPC5CUDA_FORMAT_4rVc;
-        case 8: return SPC5CUDA_FORMAT_8rVc;
-        default: return SPC5CUDA_UNDEFINED_FORMAT;
-    }
-}
-
-int vs_of(int value_type) { return value_type == SPC5CUDA_F64 ? 8 : 16; }
-int mask_bytes_of(int value_type) { return value_type == SPC5CUDA_F64 ? 1 : 2; }
-int value_bytes_of(int value_type) { return value_type == SPC5CUDA_F64 ? 8 : 4; }
-
-template <class F>
-spc5cuda_status guarded(F&& f) {
-    try {
-        f();
-        return SPC5CUDA_OK;
-    } catch (const Error& e) {
-        return e.status;
-    } catch (const std::bad_alloc&) {
-        return SPC5CUDA_ERR_NOMEM;
-    } catch (...) {
-        return SPC5CUDA_ERR_INVALID;
-    }
-}
-
-void require(bool cond, spc5cuda_status s, const char* what) {
-    if (!cond) throw Error(s, what);
-}
-
 }  // namespace
 }  // namespace spc5cuda
 
 using namespace spc5cuda;
-
-// The device-resident SPC5Mat<T> (src/spc5.hpp:44-62).
-struct spc5cuda_mat {
-    int value_type = SPC5CUDA_F64;
-    int format = SPC5CUDA_UNDEFINED_FORMAT;
-    int r = 0;
-    int nrows = 0, ncols = 0;
-    long nnz = 0;
-    long nblocks = 0;
-    Owned rowptr;   // CSR row pointer (nrows+1); dropped after conversion
-    Owned colidx;   // CSR column indices; dropped after conversion
-    Owned values;   // nnz values (CSR order, then beta order)
-    Owned brptr;    // rowsSize after conversion: ceil(nrows/r)+1 block offsets
-    Owned headers;  // blocksColumnIndexesWithMasks
-    Owned valptr;   // ceil(nrows/r)+1 value offsets (not in the reference format)
-    Owned gstart;   // ngroups+1 block-row starts of the per-group ranges
-    int ngroups = 0;
-
-    int nbr() const { return r ? div_up(nrows, r) : 0; }
-    BetaView view() const {
-        BetaView v;
-        v.r = r;
-        v.nrows = nrows;
-        v.nbr = nbr();
-        v.brptr = brptr.as<int>();
-        v.headers = headers.as<uint8_t>();
-        v.values = values.p;
-        v.valptr = valptr.as<int>();
-        v.gstart = gstart.as<int>();
-        v.ngroups = ngroups;
-        return v;
-    }
-    long device_bytes() const {
-        return long(rowptr.bytes + colidx.bytes + values.bytes + brptr.bytes + headers.bytes +
-                    valptr.bytes + gstart.bytes);
-    }
-    // The per-group block-row ranges for the current device.
-    void build_partition(cudaStream_t s) {
-        ngroups = spmv_groups(vs_of(value_type), r);
-        gstart.alloc(sizeof(int) * size_t(ngroups + 1));
-        launch_partition(nbr(), brptr.as<int>(), ngroups, gstart.as<int>(), s);
-    }
-};
 
 namespace {
 
@@ -180,8 +55,9 @@ void validate_csr(const spc5cuda_mat* m, cudaStream_t s) {
     if (h != 0) throw Error(SPC5CUDA_ERR_INVALID, "malformed CSR");
 }
 
-// Block counts per block-row -> exclusive scan into brptr; returns the total.
-long count_blocks(const spc5cuda_mat* m, int r, int* brptr_out, cudaStream_t s) {
+}  // namespace
+
+long spc5cuda::count_blocks(const spc5cuda_mat* m, int r, int* brptr_out, cudaStream_t s) {
     const long nbr = div_up(m->nrows, r);
     DevBuf tmp(sizeof(int) * size_t(scan_tmp_ints(nbr) + 1), s);
     launch_blockrow_counts(vs_of(m->value_type), r, m->nrows, m->rowptr.as<int>(),
@@ -193,13 +69,14 @@ long count_blocks(const spc5cuda_mat* m, int r, int* brptr_out, cudaStream_t s) 
     return total;
 }
 
-// Value offsets of every block-row from the header masks.
-void valptr_from_headers(int mask_bytes, int r, int nbr, const int* brptr, const uint8_t* headers,
+void spc5cuda::valptr_from_headers(int mask_bytes, int r, int nbr, const int* brptr, const uint8_t* headers,
                          int* valptr, cudaStream_t s) {
     DevBuf tmp(sizeof(int) * size_t(scan_tmp_ints(nbr) + 1), s);
     launch_blockrow_value_counts(mask_bytes, r, nbr, brptr, headers, valptr, s);
     exclusive_scan_i32(valptr, valptr, nbr, tmp.as<int>(), s);
 }
+
+namespace {
 
 template <class T>
 void core_spmv(int r, long nbRows, const int* rowsSizes, const unsigned char* headers,
@@ -482,6 +359,38 @@ spc5cuda_status spc5cuda_spmv_mixed(const spc5cuda_mat* m, const float* x, doubl
         if (m->nrows == 0) return;
         require(x && y, SPC5CUDA_ERR_INVALID, "null vector");
         launch_spmv_mixed(m->view(), x, y, static_cast<cudaStream_t>(stream));
+    });
+}
+
+spc5cuda_status spc5cuda_spmm(const spc5cuda_mat* m, int k, const void* X, long ldx, void* Y,
+                              long ldy, void* stream) {
+    return guarded([&] {
+        require(m != nullptr, SPC5CUDA_ERR_INVALID, "null");
+        require(m->r != 0, SPC5CUDA_ERR_FORMAT, "matrix is not converted");
+        require(k >= 0 && ldx >= k && ldy >= k, SPC5CUDA_ERR_INVALID, "k / leading dimensions");
+        if (m->nrows == 0 || k == 0) return;
+        require(X && Y, SPC5CUDA_ERR_INVALID, "null block of vectors");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        if (m->value_type == SPC5CUDA_F64)
+            launch_spmm_f64(m->view(), k, static_cast<const double*>(X), ldx,
+                            static_cast<double*>(Y), ldy, s);
+        else
+            launch_spmm_f32(m->view(), k, static_cast<const float*>(X), ldx,
+                            static_cast<float*>(Y), ldy, s);
+    });
+}
+
+spc5cuda_status spc5cuda_spmm_mixed(const spc5cuda_mat* m, int k, const float* X, long ldx,
+                                    double* Y, long ldy, void* stream) {
+    return guarded([&] {
+        require(m != nullptr, SPC5CUDA_ERR_INVALID, "null");
+        require(m->r != 0, SPC5CUDA_ERR_FORMAT, "matrix is not converted");
+        require(m->value_type == SPC5CUDA_F32, SPC5CUDA_ERR_FORMAT,
+                "mixed precision needs an F32 matrix");
+        require(k >= 0 && ldx >= k && ldy >= k, SPC5CUDA_ERR_INVALID, "k / leading dimensions");
+        if (m->nrows == 0 || k == 0) return;
+        require(X && Y, SPC5CUDA_ERR_INVALID, "null block of vectors");
+        launch_spmm_mixed(m->view(), k, X, ldx, Y, ldy, static_cast<cudaStream_t>(stream));
     });
 }
 

@@ -1,0 +1,171 @@
+// handle.h -- host-side internals shared by the C ABI translation units:
+// device buffers, status plumbing and the matrix handle (spc5cuda_mat).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <new>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace spc5cuda {
+
+// Stream-ordered device buffer (cudaMallocAsync / cudaFreeAsync).
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaStream_t s = nullptr;
+    DevBuf() = default;
+    DevBuf(size_t n, cudaStream_t st) : bytes(n), s(st) {
+        if (n) SPC5_CUDA(cudaMallocAsync(&p, n, st));
+    }
+    ~DevBuf() {
+        if (p) cudaFreeAsync(p, s);
+    }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+// Persistent device buffer owned by a matrix handle.
+struct Owned {
+    void* p = nullptr;
+    size_t bytes = 0;
+    void alloc(size_t n) {
+        release();
+        if (n) SPC5_CUDA(cudaMalloc(&p, n));
+        bytes = n;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    Owned() = default;
+    Owned(const Owned&) = delete;
+    Owned& operator=(const Owned&) = delete;
+    Owned(Owned&& o) noexcept : p(o.p), bytes(o.bytes) {
+        o.p = nullptr;
+        o.bytes = 0;
+    }
+    Owned& operator=(Owned&& o) noexcept {
+        if (this != &o) {
+            release();
+            p = o.p;
+            bytes = o.bytes;
+            o.p = nullptr;
+            o.bytes = 0;
+        }
+        return *this;
+    }
+    ~Owned() { release(); }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+inline bool aligned(const void* p, size_t a) { return (reinterpret_cast<uintptr_t>(p) % a) == 0; }
+
+inline int format_to_r(int format) {
+    switch (format) {
+        case SPC5CUDA_FORMAT_1rVc_WT: return 1;
+        case SPC5CUDA_FORMAT_2rVc: return 2;
+        case SPC5CUDA_FORMAT_4rVc: return 4;
+        case SPC5CUDA_FORMAT_8rVc: return 8;
+        default: return 0;
+    }
+}
+
+inline int r_to_format(int r) {
+    switch (r) {
+        case 1: return SPC5CUDA_FORMAT_1rVc_WT;
+        case 2: return SPC5CUDA_FORMAT_2rVc;
+        case 4: return SPC5CUDA_FORMAT_4rVc;
+        case 8: return SPC5CUDA_FORMAT_8rVc;
+        default: return SPC5CUDA_UNDEFINED_FORMAT;
+    }
+}
+
+inline int vs_of(int value_type) { return value_type == SPC5CUDA_F64 ? 8 : 16; }
+inline int mask_bytes_of(int value_type) { return value_type == SPC5CUDA_F64 ? 1 : 2; }
+inline int value_bytes_of(int value_type) { return value_type == SPC5CUDA_F64 ? 8 : 4; }
+
+template <class F>
+inline spc5cuda_status guarded(F&& f) {
+    try {
+        f();
+        return SPC5CUDA_OK;
+    } catch (const Error& e) {
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        return SPC5CUDA_ERR_NOMEM;
+    } catch (...) {
+        return SPC5CUDA_ERR_INVALID;
+    }
+}
+
+inline void require(bool cond, spc5cuda_status s, const char* what) {
+    if (!cond) throw Error(s, what);
+}
+
+
+}  // namespace spc5cuda
+
+// The device-resident SPC5Mat<T> (src/spc5.hpp:44-62).
+struct spc5cuda_mat {
+    using Owned = spc5cuda::Owned;
+    using BetaView = spc5cuda::BetaView;
+    int value_type = SPC5CUDA_F64;
+    int format = SPC5CUDA_UNDEFINED_FORMAT;
+    int r = 0;
+    int nrows = 0, ncols = 0;
+    long nnz = 0;
+    long nblocks = 0;
+    Owned rowptr;   // CSR row pointer (nrows+1); dropped after conversion
+    Owned colidx;   // CSR column indices; dropped after conversion
+    Owned values;   // nnz values (CSR order, then beta order)
+    Owned brptr;    // rowsSize after conversion: ceil(nrows/r)+1 block offsets
+    Owned headers;  // blocksColumnIndexesWithMasks
+    Owned valptr;   // ceil(nrows/r)+1 value offsets (not in the reference format)
+    Owned gstart;   // ngroups+1 block-row starts of the per-group ranges
+    int ngroups = 0;
+
+    int nbr() const { return r ? spc5cuda::div_up(nrows, r) : 0; }
+    BetaView view() const {
+        BetaView v;
+        v.r = r;
+        v.nrows = nrows;
+        v.nbr = nbr();
+        v.brptr = brptr.as<int>();
+        v.headers = headers.as<uint8_t>();
+        v.values = values.p;
+        v.valptr = valptr.as<int>();
+        v.gstart = gstart.as<int>();
+        v.ngroups = ngroups;
+        return v;
+    }
+    long device_bytes() const {
+        return long(rowptr.bytes + colidx.bytes + values.bytes + brptr.bytes + headers.bytes +
+                    valptr.bytes + gstart.bytes);
+    }
+    // The per-group block-row ranges for the current device.
+    void build_partition(cudaStream_t s) {
+        ngroups = spc5cuda::spmv_groups(spc5cuda::vs_of(value_type), r);
+        gstart.alloc(sizeof(int) * size_t(ngroups + 1));
+        spc5cuda::launch_partition(nbr(), brptr.as<int>(), ngroups, gstart.as<int>(), s);
+    }
+};
+
+
+namespace spc5cuda {
+
+// Block counts per block-row of a CSR handle for rows-per-block r, scanned
+// into brptr_out (ceil(nrows/r)+1 ints); returns the total (synchronises s).
+long count_blocks(const spc5cuda_mat* m, int r, int* brptr_out, cudaStream_t s);
+
+// Value offsets of every block-row from the header masks.
+void valptr_from_headers(int mask_bytes, int r, int nbr, const int* brptr, const uint8_t* headers,
+                         int* valptr, cudaStream_t s);
+
+}  // namespace spc5cuda

@@ -60,4 +60,37 @@ void launch_spmv_f64(const BetaView& m, const double* x, double* y, cudaStream_t
 void launch_spmv_f32(const BetaView& m, const float* x, float* y, cudaStream_t s);
 void launch_spmv_mixed(const BetaView& m, const float* x, double* y, cudaStream_t s);
 
+// ---- SpMM (spmm.cu): Y += A X, row-major X (ncols x k, ldx) and Y (nrows x k, ldy)
+void launch_spmm_f64(const BetaView& m, int k, const double* x, long ldx, double* y, long ldy,
+                     cudaStream_t s);
+void launch_spmm_f32(const BetaView& m, int k, const float* x, long ldx, float* y, long ldy,
+                     cudaStream_t s);
+void launch_spmm_mixed(const BetaView& m, int k, const float* x, long ldx, double* y, long ldy,
+                       cudaStream_t s);
+
+// ---- batched SpMM (spmm.cu): many matrices, one launch per (r, kc) class
+struct BatchMat {
+    const int* brptr;
+    const uint8_t* headers;
+    const void* values;
+    const int* valptr;
+    const void* x;  // row-major ncols x k (ldx)
+    long ldx;
+    void* y;        // row-major nrows x k (ldy)
+    long ldy;
+    int nrows;
+    int pad;
+};
+struct BatchJob {
+    int mat;      // index into the BatchMat array
+    int r_begin;  // block-row range
+    int r_end;
+    int kofs;     // first right-hand side of this pass
+};
+// right-hand sides per pass for rows-per-block r and k right-hand sides
+int batch_kc(int r, int k);
+// kind 0 = f64, 1 = f32, 2 = mixed (f32 values and x, f64 y)
+void launch_batch(int kind, int r, int kc, const BatchMat* mats, const BatchJob* jobs, int njobs,
+                  int ctas, cudaStream_t s);
+
 }  // namespace spc5cuda

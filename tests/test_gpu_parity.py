@@ -208,3 +208,94 @@ def test_full_size_bit_exact(cuda, which):
         y = gpu_spmv(m, x, np.zeros(csr.nrows))
         assert y.tobytes() == yo.tobytes()
         del m
+
+
+@pytest.mark.parametrize("tag,dt", DTYPES)
+@pytest.mark.parametrize("r", [1, 2, 4, 8])
+@pytest.mark.parametrize("k", [1, 3, 4, 8, 16])
+def test_spmm_columns_equal_spmv(cuda, tag, dt, r, k):
+    """Every column of Y += A X equals an independent SpMV of that column,
+    bit for bit (the request loop relies on it)."""
+    for csr in list(irregular_cases())[:4]:
+        m = converted(csr, dt, r)
+        X = np.stack([M.x_vector(csr.ncols, 30 + j, dt) for j in range(k)], axis=1)
+        Y0 = np.stack([M.x_vector(csr.nrows, 60 + j, dt) for j in range(k)], axis=1)
+        Yd = dev(Y0)
+        S.SPC5_Spmm(m, dev(X), Yd)
+        torch.cuda.synchronize()
+        Y = Yd.cpu().numpy()
+        for j in range(k):
+            yj = gpu_spmv(m, np.ascontiguousarray(X[:, j]), np.ascontiguousarray(Y0[:, j]))
+            assert Y[:, j].tobytes() == yj.tobytes(), (csr.name, j)
+
+
+@pytest.mark.parametrize("r", [1, 4, 8])
+def test_spmm_mixed_columns(cuda, r):
+    csr = M.powerlaw(5000, seed=12)
+    m = converted(csr, np.float32, r)
+    k = 5
+    X = np.stack([M.x_vector(csr.ncols, 40 + j, np.float32) for j in range(k)], axis=1)
+    Yd = torch.zeros(csr.nrows, k, dtype=torch.float64, device="cuda")
+    S.SPC5_Spmm_mixed(m, dev(X), Yd)
+    torch.cuda.synchronize()
+    brptr, headers, v32 = m.arrays()
+    for j in range(k):
+        yo = oracle.beta_spmv_mixed(r, csr.nrows, brptr, headers, v32, np.ascontiguousarray(X[:, j]),
+                                    np.zeros(csr.nrows))
+        assert Yd[:, j].cpu().numpy().tobytes() == yo.tobytes()
+
+
+def test_find_best_matches_reference(cuda, golden):
+    """SPC5_find_best on device block counts picks the reference's format."""
+    for n in names(golden):
+        csr = golden_csr(golden, n)
+        m = S.csr_matrix(csr.rowptr, csr.colidx, csr.values, csr.ncols)
+        r, est = S.SPC5_find_best(m)
+        assert r == int(golden[f"{n}/find_best_r"]), n
+        assert est == pytest.approx(float(golden[f"{n}/find_best_est"]), rel=1e-12), n
+
+
+@pytest.mark.parametrize("mode", [S.TUNE_MODEL, S.TUNE_MEASURE])
+def test_autotune(cuda, mode):
+    for csr in (M.stencil27(20), M.powerlaw(30000, seed=4), M.banded(5000, 30, 0.2, seed=2)):
+        m = S.csr_matrix(csr.rowptr, csr.colidx, csr.values, csr.ncols)
+        t = S.autotune(m, mode)
+        assert t["r"] in (1, 2, 4, 8)
+        for r in (1, 2, 4, 8):
+            assert t["blocks"][r] == oracle.block_count(r, csr.rowptr, csr.colidx)
+            assert t["est_us"][r] > 0
+        assert t["est_us"][t["r"]] == min(t["est_us"].values())
+        assert m.format == S.FORMAT_CSR  # the autotuner leaves the handle untouched
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_batch_equals_independent_spmv(cuda, mixed):
+    """One graph over matrices of uneven sizes, r and k: every column equals
+    the independent SpMV bit for bit."""
+    rng = np.random.default_rng(5)
+    mats, Xs, Ys, keep = [], [], [], []
+    dt = np.float32 if mixed else np.float64
+    for i in range(12):
+        n = int(rng.integers(50, 6000))
+        csr = M.banded(n, int(rng.integers(2, 60)), 0.3, seed=100 + i)
+        r = (1, 2, 4, 8)[i % 4]
+        k = (1, 4, 8, 16, 3)[i % 5]
+        m = converted(csr, dt, r)
+        X = dev(np.stack([M.x_vector(n, 200 + i * 20 + j, dt) for j in range(k)], axis=1))
+        Y = torch.zeros(n, k, dtype=torch.float64 if mixed or dt == np.float64 else torch.float32,
+                        device="cuda")
+        mats.append(m); Xs.append(X); Ys.append(Y); keep.append((csr, r))
+    b = S.Batch(mats, Xs, Ys, mixed=mixed)
+    nclasses, njobs = b.info()
+    assert nclasses >= 4 and njobs >= 12
+    for _ in range(2):  # y accumulates over two replays
+        b.launch()
+    torch.cuda.synchronize()
+    for m, X, Y, (csr, r) in zip(mats, Xs, Ys, keep):
+        for j in range(X.shape[1]):
+            y = torch.zeros(csr.nrows, dtype=Y.dtype, device="cuda")
+            xj = X[:, j].contiguous()
+            for _ in range(2):
+                (S.SPC5_Spmv_mixed if mixed else S.SPC5_Spmv)(m, xj, y)
+            torch.cuda.synchronize()
+            assert Y[:, j].cpu().numpy().tobytes() == y.cpu().numpy().tobytes(), (csr.name, r, j)
