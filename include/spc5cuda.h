@@ -237,6 +237,57 @@ SPC5CUDA_API spc5cuda_status spc5cuda_batch_info(const spc5cuda_batch* batch, in
                                                  long* njobs);
 SPC5CUDA_API spc5cuda_status spc5cuda_batch_destroy(spc5cuda_batch* batch);
 
+/* ------------------------------------------------------------------------
+ * Request loop (no counterpart in the reference): resident matrices,
+ * admission by HBM footprint, same-matrix requests coalesced into
+ * multi-RHS launches (k <= max_k), up to `slots` launches in flight
+ * (continuous batching), latency percentiles.  A request computes
+ * y = A_id x for DEVICE vectors x (ncols) and y (nrows) that stay valid until
+ * the request completes.  Each result is bit-identical to a solo SpMV.
+ * ---------------------------------------------------------------------- */
+typedef struct spc5cuda_server spc5cuda_server;
+
+typedef struct spc5cuda_server_config {
+    int slots;        /* concurrent launches (streams), 1..64             */
+    int max_k;        /* requests coalesced per launch, 1..16             */
+    long hbm_budget;  /* bytes for resident matrices + staging buffers    */
+    int mixed;        /* 0: F64 matrices, double x/y; 1: F32 matrices,
+                         float x, double y (FP64 accumulation)            */
+    int pad;
+} spc5cuda_server_config;
+
+typedef struct spc5cuda_server_stats {
+    long completed;      /* requests completed since the last reset          */
+    long launches;       /* SpMM launches                                    */
+    double mean_k;       /* requests per launch                              */
+    double p50_us;       /* submit -> completion latency percentiles         */
+    double p99_us;
+    double max_us;
+    double req_per_s;    /* completed / (last completion - first submit)     */
+    long resident_bytes; /* device bytes of the registered matrices          */
+    int matrices;
+    int pad;
+} spc5cuda_server_stats;
+
+SPC5CUDA_API spc5cuda_status spc5cuda_server_create(spc5cuda_server** out,
+                                                    const spc5cuda_server_config* cfg);
+/* Registers a converted matrix (the handle stays owned by the caller and
+ * must outlive the server).  SPC5CUDA_ERR_NOMEM when the resident bytes
+ * plus staging would exceed the HBM budget.  Only while no request is in
+ * flight. */
+SPC5CUDA_API spc5cuda_status spc5cuda_server_add_matrix(spc5cuda_server* srv, spc5cuda_mat* mat,
+                                                        int* id);
+SPC5CUDA_API spc5cuda_status spc5cuda_server_submit(spc5cuda_server* srv, int id, const void* x,
+                                                    void* y, long* request);
+/* Blocks until the request completes (SPC5CUDA_ERR_TIMEOUT after timeout_s);
+ * latency_us may be NULL.  A request can be waited on once. */
+SPC5CUDA_API spc5cuda_status spc5cuda_server_wait(spc5cuda_server* srv, long request,
+                                                  double timeout_s, double* latency_us);
+SPC5CUDA_API spc5cuda_status spc5cuda_server_drain(spc5cuda_server* srv, double timeout_s);
+SPC5CUDA_API spc5cuda_status spc5cuda_server_get_stats(spc5cuda_server* srv,
+                                                   spc5cuda_server_stats* out, int reset);
+SPC5CUDA_API spc5cuda_status spc5cuda_server_destroy(spc5cuda_server* srv);
+
 #ifdef __cplusplus
 }
 #endif

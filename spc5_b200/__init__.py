@@ -45,7 +45,9 @@ EXPORTED_SYMBOLS = [
     "spc5cuda_mat_info", "spc5cuda_block_count", "spc5cuda_convert", "spc5cuda_get_arrays",
     "spc5cuda_spmv", "spc5cuda_spmv_mixed", "spc5cuda_spmm", "spc5cuda_spmm_mixed",
     "spc5cuda_find_best", "spc5cuda_autotune", "spc5cuda_batch_create", "spc5cuda_batch_launch",
-    "spc5cuda_batch_info", "spc5cuda_batch_destroy",
+    "spc5cuda_batch_info", "spc5cuda_batch_destroy", "spc5cuda_server_create",
+    "spc5cuda_server_add_matrix", "spc5cuda_server_submit", "spc5cuda_server_wait",
+    "spc5cuda_server_drain", "spc5cuda_server_get_stats", "spc5cuda_server_destroy",
 ]
 
 TUNE_MODEL = 0
@@ -61,6 +63,18 @@ class SPC5Error(RuntimeError):
 
 class spc5cuda_tune(C.Structure):
     _fields_ = [("r", C.c_int), ("pad", C.c_int), ("blocks", C.c_long * 4), ("est_us", C.c_double * 4)]
+
+
+class spc5cuda_server_config(C.Structure):
+    _fields_ = [("slots", C.c_int), ("max_k", C.c_int), ("hbm_budget", C.c_long), ("mixed", C.c_int),
+                ("pad", C.c_int)]
+
+
+class spc5cuda_server_stats(C.Structure):
+    _fields_ = [("completed", C.c_long), ("launches", C.c_long), ("mean_k", C.c_double),
+                ("p50_us", C.c_double), ("p99_us", C.c_double), ("max_us", C.c_double),
+                ("req_per_s", C.c_double), ("resident_bytes", C.c_long), ("matrices", C.c_int),
+                ("pad", C.c_int)]
 
 
 class spc5cuda_info(C.Structure):
@@ -130,6 +144,20 @@ def _lib():
         lib.spc5cuda_batch_info.argtypes = [_P, C.POINTER(_I), C.POINTER(_L)]
         lib.spc5cuda_batch_destroy.restype = _I
         lib.spc5cuda_batch_destroy.argtypes = [_P]
+        lib.spc5cuda_server_create.restype = _I
+        lib.spc5cuda_server_create.argtypes = [C.POINTER(_P), C.POINTER(spc5cuda_server_config)]
+        lib.spc5cuda_server_add_matrix.restype = _I
+        lib.spc5cuda_server_add_matrix.argtypes = [_P, _P, C.POINTER(_I)]
+        lib.spc5cuda_server_submit.restype = _I
+        lib.spc5cuda_server_submit.argtypes = [_P, _I, _P, _P, C.POINTER(_L)]
+        lib.spc5cuda_server_wait.restype = _I
+        lib.spc5cuda_server_wait.argtypes = [_P, _L, C.c_double, C.POINTER(C.c_double)]
+        lib.spc5cuda_server_drain.restype = _I
+        lib.spc5cuda_server_drain.argtypes = [_P, C.c_double]
+        lib.spc5cuda_server_get_stats.restype = _I
+        lib.spc5cuda_server_get_stats.argtypes = [_P, C.POINTER(spc5cuda_server_stats), _I]
+        lib.spc5cuda_server_destroy.restype = _I
+        lib.spc5cuda_server_destroy.argtypes = [_P]
         _LIB = lib
     return _LIB
 
@@ -416,6 +444,62 @@ class Batch:
         if h and _LIB is not None:
             _LIB.spc5cuda_batch_destroy(h)
             self._h = None
+
+
+class Server:
+    """Request loop over resident matrices (continuous batching of
+    same-matrix requests into multi-RHS launches, admission by HBM footprint,
+    latency percentiles).  A request computes y = A x for device tensors."""
+
+    def __init__(self, slots=4, max_k=16, hbm_budget=None, mixed=False):
+        import torch
+        if hbm_budget is None:
+            free, _ = torch.cuda.mem_get_info()
+            hbm_budget = int(free * 0.9)
+        cfg = spc5cuda_server_config(int(slots), int(max_k), int(hbm_budget), 1 if mixed else 0, 0)
+        self.mixed = bool(mixed)
+        self._h = C.c_void_p()
+        self._mats = []
+        self._live = {}
+        _check(_lib().spc5cuda_server_create(C.byref(self._h), C.byref(cfg)), "spc5cuda_server_create")
+
+    def add_matrix(self, mat: SPC5Mat) -> int:
+        i = C.c_int(-1)
+        _check(_lib().spc5cuda_server_add_matrix(self._h, mat.handle, C.byref(i)), "add_matrix")
+        self._mats.append(mat)
+        return int(i.value)
+
+    def submit(self, mat_id: int, x, y) -> int:
+        """Queues y = A_mat_id x (x, y CUDA tensors kept alive until wait/drain)."""
+        rid = C.c_long(0)
+        _check(_lib().spc5cuda_server_submit(self._h, int(mat_id), C.c_void_p(x.data_ptr()),
+                                             C.c_void_p(y.data_ptr()), C.byref(rid)), "submit")
+        self._live[int(rid.value)] = (x, y)
+        return int(rid.value)
+
+    def wait(self, rid: int, timeout_s: float = 60.0) -> float:
+        lat = C.c_double(0.0)
+        _check(_lib().spc5cuda_server_wait(self._h, int(rid), float(timeout_s), C.byref(lat)), "wait")
+        self._live.pop(int(rid), None)
+        return float(lat.value)
+
+    def drain(self, timeout_s: float = 120.0) -> None:
+        _check(_lib().spc5cuda_server_drain(self._h, float(timeout_s)), "drain")
+        self._live.clear()
+
+    def stats(self, reset: bool = False) -> dict:
+        st = spc5cuda_server_stats()
+        _check(_lib().spc5cuda_server_get_stats(self._h, C.byref(st), 1 if reset else 0), "stats")
+        return {f[0]: getattr(st, f[0]) for f in st._fields_ if f[0] != "pad"}
+
+    def close(self) -> None:
+        h = getattr(self, "_h", None)
+        if h and _LIB is not None:
+            _LIB.spc5cuda_server_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
 
 
 def core_spmv(r: int, nbRows: int, rowsSizes, headers, values, x, y, stream=None) -> None:

@@ -69,6 +69,8 @@ spc5cuda_status spc5cuda_batch_create(spc5cuda_batch** out, int n, spc5cuda_mat*
                 b.ldx = ldx[i];
                 b.y = Y[i];
                 b.ldy = ldy[i];
+                b.xcs = 1;
+                b.ycs = 1;
                 b.nrows = m->nrows;
                 b.pad = 0;
                 if (m->nrows == 0 || k[i] == 0) continue;

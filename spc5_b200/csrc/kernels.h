@@ -60,13 +60,15 @@ void launch_spmv_f64(const BetaView& m, const double* x, double* y, cudaStream_t
 void launch_spmv_f32(const BetaView& m, const float* x, float* y, cudaStream_t s);
 void launch_spmv_mixed(const BetaView& m, const float* x, double* y, cudaStream_t s);
 
-// ---- SpMM (spmm.cu): Y += A X, row-major X (ncols x k, ldx) and Y (nrows x k, ldy)
-void launch_spmm_f64(const BetaView& m, int k, const double* x, long ldx, double* y, long ldy,
-                     cudaStream_t s);
-void launch_spmm_f32(const BetaView& m, int k, const float* x, long ldx, float* y, long ldy,
-                     cudaStream_t s);
-void launch_spmm_mixed(const BetaView& m, int k, const float* x, long ldx, double* y, long ldy,
-                       cudaStream_t s);
+// ---- SpMM (spmm.cu): Y += A X.  Element (row i, right-hand side q) of X
+// is x[i * ldx + q * xcs] (row-major: xcs = 1; column-major: ldx = 1,
+// xcs = leading dimension), likewise Y with ldy, ycs.
+void launch_spmm_f64(const BetaView& m, int k, const double* x, long ldx, long xcs, double* y,
+                     long ldy, long ycs, cudaStream_t s);
+void launch_spmm_f32(const BetaView& m, int k, const float* x, long ldx, long xcs, float* y,
+                     long ldy, long ycs, cudaStream_t s);
+void launch_spmm_mixed(const BetaView& m, int k, const float* x, long ldx, long xcs, double* y,
+                       long ldy, long ycs, cudaStream_t s);
 
 // ---- batched SpMM (spmm.cu): many matrices, one launch per (r, kc) class
 struct BatchMat {
@@ -78,6 +80,8 @@ struct BatchMat {
     long ldx;
     void* y;        // row-major nrows x k (ldy)
     long ldy;
+    long xcs;       // stride between right-hand sides (1: row-major)
+    long ycs;
     int nrows;
     int pad;
 };

@@ -28,7 +28,7 @@ __device__ __forceinline__ void spmm_range(bool has, int nrows, const int* __res
                                            const uint8_t* __restrict__ headers,
                                            const V* __restrict__ values, int r_begin, int r_end,
                                            int v_begin, const X* __restrict__ xm, long ldx,
-                                           Y* __restrict__ ym, long ldy) {
+                                           long xcs, Y* __restrict__ ym, long ldy, long ycs) {
     constexpr int VS = Layout<LT>::VS;
     using H = Header<LT, R>;
     constexpr int MW = H::MASK_WORDS;
@@ -63,7 +63,7 @@ __device__ __forceinline__ void spmm_range(bool has, int nrows, const int* __res
                     for (int d = VS / 2; d >= 1; d >>= 1) s += __shfl_xor_sync(FULL, s, d, VS);
                     const int yrow = row * R + i;
                     if (need && ((i * KC + q) % VS) == c && yrow < nrows) {
-                        Y* dst = ym + long(yrow) * ldy + q;
+                        Y* dst = ym + long(yrow) * ldy + long(q) * ycs;
                         if constexpr (sizeof(Y) == 8) atomicAdd(dst, Y(s));
                         else *dst = *dst + Y(s);
                     }
@@ -114,7 +114,7 @@ __device__ __forceinline__ void spmm_range(bool has, int nrows, const int* __res
             A xk[KC];
             const X* xr = xm + long(bcol + c) * ldx;
 #pragma unroll
-            for (int q = 0; q < KC; ++q) xk[q] = A(__ldg(xr + q));
+            for (int q = 0; q < KC; ++q) xk[q] = A(__ldg(xr + long(q) * xcs));
             int pre = bv;
 #pragma unroll
             for (int i = 0; i < R; ++i) {
@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(128)
     k_spmm(int nrows, const int* __restrict__ brptr, const uint8_t* __restrict__ headers,
            const V* __restrict__ values, const int* __restrict__ valptr,
            const int* __restrict__ gstart, int ngroups, const X* __restrict__ xm, long ldx,
-           Y* __restrict__ ym, long ldy) {
+           long xcs, Y* __restrict__ ym, long ldy, long ycs) {
     constexpr int VS = Layout<LT>::VS;
     const int group = int((long(blockIdx.x) * blockDim.x + threadIdx.x) / VS);
     int r_begin = 0, r_end = 0;
@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(128)
     const bool has = r_begin < r_end;
     const int v_begin = has ? __ldg(valptr + r_begin) : 0;
     spmm_range<LT, R, KC, V, X, A, Y>(has, nrows, brptr, headers, values, r_begin, r_end, v_begin,
-                                      xm, ldx, ym, ldy);
+                                      xm, ldx, xcs, ym, ldy, ycs);
 }
 
 // Batched launch: job j is block-rows [r_begin, r_end) of matrix mats[j.mat]
@@ -181,8 +181,8 @@ __global__ void __launch_bounds__(128)
         const int v_begin = has ? __ldg(m.valptr + job.r_begin) : 0;
         spmm_range<LT, R, KC, V, X, A, Y>(
             has, m.nrows, m.brptr, m.headers, static_cast<const V*>(m.values), job.r_begin, job.r_end,
-            v_begin, static_cast<const X*>(m.x) + job.kofs, m.ldx, static_cast<Y*>(m.y) + job.kofs,
-            m.ldy);
+            v_begin, static_cast<const X*>(m.x) + long(job.kofs) * m.xcs, m.ldx, m.xcs,
+            static_cast<Y*>(m.y) + long(job.kofs) * m.ycs, m.ldy, m.ycs);
     }
 }
 
@@ -194,37 +194,40 @@ constexpr int kc_max() {
 }
 
 template <class LT, int R, int KC, class V, class X, class A, class Y>
-void launch_kc(const BetaView& m, const X* x, long ldx, Y* y, long ldy, cudaStream_t s) {
+void launch_kc(const BetaView& m, const X* x, long ldx, long xcs, Y* y, long ldy, long ycs,
+               cudaStream_t s) {
     constexpr int VS = Layout<LT>::VS;
     const int threads = 128;
     const int ctas = int((long(m.ngroups) * VS + threads - 1) / threads);
     k_spmm<LT, R, KC, V, X, A, Y><<<ctas, threads, 0, s>>>(m.nrows, m.brptr, m.headers,
                                                             static_cast<const V*>(m.values), m.valptr,
-                                                            m.gstart, m.ngroups, x, ldx, y, ldy);
+                                                            m.gstart, m.ngroups, x, ldx, xcs, y, ldy,
+                                                            ycs);
 }
 
 template <class LT, int R, class V, class X, class A, class Y>
-void launch_r(const BetaView& m, int k, const X* x, long ldx, Y* y, long ldy, cudaStream_t s) {
+void launch_r(const BetaView& m, int k, const X* x, long ldx, long xcs, Y* y, long ldy, long ycs,
+              cudaStream_t s) {
     constexpr int KMAX = kc_max<R>();
     int k0 = 0;
     while (k0 < k) {
         const int rem = k - k0;
-        const X* xs = x + k0;
-        Y* ys = y + k0;
+        const X* xs = x + long(k0) * xcs;
+        Y* ys = y + long(k0) * ycs;
         if (rem >= KMAX) {
-            launch_kc<LT, R, KMAX, V, X, A, Y>(m, xs, ldx, ys, ldy, s);
+            launch_kc<LT, R, KMAX, V, X, A, Y>(m, xs, ldx, xcs, ys, ldy, ycs, s);
             k0 += KMAX;
         } else if (rem >= 8 && KMAX >= 8) {
-            launch_kc<LT, R, (KMAX >= 8 ? 8 : 1), V, X, A, Y>(m, xs, ldx, ys, ldy, s);
+            launch_kc<LT, R, (KMAX >= 8 ? 8 : 1), V, X, A, Y>(m, xs, ldx, xcs, ys, ldy, ycs, s);
             k0 += 8;
         } else if (rem >= 4) {
-            launch_kc<LT, R, 4, V, X, A, Y>(m, xs, ldx, ys, ldy, s);
+            launch_kc<LT, R, 4, V, X, A, Y>(m, xs, ldx, xcs, ys, ldy, ycs, s);
             k0 += 4;
         } else if (rem >= 2) {
-            launch_kc<LT, R, 2, V, X, A, Y>(m, xs, ldx, ys, ldy, s);
+            launch_kc<LT, R, 2, V, X, A, Y>(m, xs, ldx, xcs, ys, ldy, ycs, s);
             k0 += 2;
         } else {
-            launch_kc<LT, R, 1, V, X, A, Y>(m, xs, ldx, ys, ldy, s);
+            launch_kc<LT, R, 1, V, X, A, Y>(m, xs, ldx, xcs, ys, ldy, ycs, s);
             k0 += 1;
         }
     }
@@ -232,33 +235,33 @@ void launch_r(const BetaView& m, int k, const X* x, long ldx, Y* y, long ldy, cu
 }
 
 template <class LT, class V, class X, class A, class Y>
-void launch_spmm_impl(const BetaView& m, int k, const X* x, long ldx, Y* y, long ldy,
-                      cudaStream_t s) {
+void launch_spmm_impl(const BetaView& m, int k, const X* x, long ldx, long xcs, Y* y, long ldy,
+                      long ycs, cudaStream_t s) {
     if (m.nbr <= 0 || k <= 0) return;
     switch (m.r) {
-        case 1: launch_r<LT, 1, V, X, A, Y>(m, k, x, ldx, y, ldy, s); break;
-        case 2: launch_r<LT, 2, V, X, A, Y>(m, k, x, ldx, y, ldy, s); break;
-        case 4: launch_r<LT, 4, V, X, A, Y>(m, k, x, ldx, y, ldy, s); break;
-        case 8: launch_r<LT, 8, V, X, A, Y>(m, k, x, ldx, y, ldy, s); break;
+        case 1: launch_r<LT, 1, V, X, A, Y>(m, k, x, ldx, xcs, y, ldy, ycs, s); break;
+        case 2: launch_r<LT, 2, V, X, A, Y>(m, k, x, ldx, xcs, y, ldy, ycs, s); break;
+        case 4: launch_r<LT, 4, V, X, A, Y>(m, k, x, ldx, xcs, y, ldy, ycs, s); break;
+        case 8: launch_r<LT, 8, V, X, A, Y>(m, k, x, ldx, xcs, y, ldy, ycs, s); break;
         default: throw Error(SPC5CUDA_ERR_FORMAT, "r must be 1, 2, 4 or 8");
     }
 }
 
 }  // namespace
 
-void launch_spmm_f64(const BetaView& m, int k, const double* x, long ldx, double* y, long ldy,
-                     cudaStream_t s) {
-    launch_spmm_impl<double, double, double, double, double>(m, k, x, ldx, y, ldy, s);
+void launch_spmm_f64(const BetaView& m, int k, const double* x, long ldx, long xcs, double* y,
+                     long ldy, long ycs, cudaStream_t s) {
+    launch_spmm_impl<double, double, double, double, double>(m, k, x, ldx, xcs, y, ldy, ycs, s);
 }
 
-void launch_spmm_f32(const BetaView& m, int k, const float* x, long ldx, float* y, long ldy,
-                     cudaStream_t s) {
-    launch_spmm_impl<float, float, float, float, float>(m, k, x, ldx, y, ldy, s);
+void launch_spmm_f32(const BetaView& m, int k, const float* x, long ldx, long xcs, float* y,
+                     long ldy, long ycs, cudaStream_t s) {
+    launch_spmm_impl<float, float, float, float, float>(m, k, x, ldx, xcs, y, ldy, ycs, s);
 }
 
-void launch_spmm_mixed(const BetaView& m, int k, const float* x, long ldx, double* y, long ldy,
-                       cudaStream_t s) {
-    launch_spmm_impl<float, float, float, double, double>(m, k, x, ldx, y, ldy, s);
+void launch_spmm_mixed(const BetaView& m, int k, const float* x, long ldx, long xcs, double* y,
+                       long ldy, long ycs, cudaStream_t s) {
+    launch_spmm_impl<float, float, float, double, double>(m, k, x, ldx, xcs, y, ldy, ycs, s);
 }
 
 int batch_kc(int r, int k) {

@@ -1,0 +1,81 @@
+"""The request loop: continuous batching over resident matrices.
+
+Each request's result must be identical, bit for bit, whether it runs alone
+or coalesced with other requests to the same matrix while other launches
+overlap on the device; admission by HBM footprint must reject a matrix that
+does not fit the budget.
+"""
+import numpy as np
+import pytest
+import torch
+
+import spc5_b200 as S
+from spc5_b200 import matrices as M
+
+pytestmark = pytest.mark.gpu
+
+
+def converted(csr, dt, r):
+    m = S.csr_matrix(csr.rowptr, csr.colidx, csr.values.astype(dt), csr.ncols)
+    S.CSR_to_SPC5(m, S.FORMAT_OF_R[r])
+    return m
+
+
+def solo(m, x, mixed):
+    y = torch.zeros(m.numberOfRows, dtype=torch.float64, device="cuda")
+    (S.SPC5_Spmv_mixed if mixed else S.SPC5_Spmv)(m, x, y)
+    torch.cuda.synchronize()
+    return y
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_results_same_alone_and_in_the_mix(cuda, mixed):
+    dt = np.float32 if mixed else np.float64
+    tdt = torch.float32 if mixed else torch.float64
+    csrs = [M.powerlaw(20000, seed=3), M.stencil27(18), M.banded(7000, 40, 0.2, seed=5)]
+    mats = [converted(c, dt, r) for c, r in zip(csrs, (1, 4, 2))]
+    srv = S.Server(slots=3, max_k=16, mixed=mixed)
+    ids = [srv.add_matrix(m) for m in mats]
+    rng = np.random.default_rng(0)
+    reqs = []
+    for q in range(300):
+        i = int(rng.integers(0, len(mats)))
+        x = torch.from_numpy(M.x_vector(csrs[i].ncols, 1000 + q, dt)).cuda()
+        y = torch.full((csrs[i].nrows,), float("nan"), dtype=torch.float64, device="cuda")
+        reqs.append((i, x, y, srv.submit(ids[i], x, y)))
+    for _, _, _, rid in reqs:
+        assert srv.wait(rid) >= 0.0
+    st = srv.stats()
+    assert st["completed"] == 300 and st["launches"] < 300 and st["mean_k"] > 1.0
+    assert st["p99_us"] >= st["p50_us"] > 0
+    for i, x, y, _ in reqs:
+        assert y.cpu().numpy().tobytes() == solo(mats[i], x, mixed).cpu().numpy().tobytes()
+    # alone: one request at a time
+    for i, x, y, _ in reqs[:20]:
+        y2 = torch.empty_like(y)
+        srv.wait(srv.submit(ids[i], x, y2))
+        assert y2.cpu().numpy().tobytes() == y.cpu().numpy().tobytes()
+    srv.close()
+    del tdt
+
+
+def test_admission_by_hbm_footprint(cuda):
+    csr = M.stencil27(20)
+    m = converted(csr, np.float64, 4)
+    small = S.Server(slots=2, max_k=4, hbm_budget=m.info().device_bytes // 2)
+    with pytest.raises(S.SPC5Error) as e:
+        small.add_matrix(m)
+    assert e.value.status == 3
+    ok = S.Server(slots=2, max_k=4, hbm_budget=1 << 30)
+    assert ok.add_matrix(m) == 0
+    assert ok.stats()["resident_bytes"] == m.info().device_bytes
+    small.close()
+    ok.close()
+
+
+def test_wrong_value_type_rejected(cuda):
+    m = converted(M.poisson2d(16), np.float64, 2)
+    srv = S.Server(slots=1, max_k=2, hbm_budget=1 << 28, mixed=True)
+    with pytest.raises(S.SPC5Error):
+        srv.add_matrix(m)
+    srv.close()
