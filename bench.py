@@ -394,13 +394,179 @@ def run_gpu(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# batched workload: many banded matrices, per-matrix r, k right-hand sides
+# ---------------------------------------------------------------------------
+
+def batched_matrices(count=256, seed=3):
+    """Banded matrices with N log-uniform in [2e3, 2e5], bandwidth U[5, 200],
+    density 0.1 in the band, values U[-1, 1]; k in {1, 4, 8, 16}."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(2e3), np.log(2e5)))))
+        bw = int(rng.integers(5, 201))
+        k = int(rng.choice([1, 4, 8, 16]))
+        out.append((M.banded(n, bw, 0.1, seed=seed * 100003 + i), k))
+    return out
+
+
+def run_batched(args):
+    import torch
+
+    import spc5_b200 as S
+    torch.cuda.set_device(0)
+    work = batched_matrices(args.batch_count)
+    lines = []
+    for mixed in (False, True):
+        dt = np.float32 if mixed else np.float64
+        tdt = torch.float32 if mixed else torch.float64
+        mats, Xs, Ys, total_bytes, flops, chosen = [], [], [], 0, 0, {}
+        for csr, k in work:
+            m = S.csr_matrix(csr.rowptr, csr.colidx, csr.values.astype(dt), csr.ncols)
+            r = S.autotune(m, S.TUNE_MODEL)["r"]
+            S.CSR_to_SPC5(m, S.FORMAT_OF_R[r])
+            chosen[r] = chosen.get(r, 0) + 1
+            mats.append(m)
+            Xs.append(torch.from_numpy(np.random.default_rng(len(Xs)).uniform(-1, 1, (csr.ncols, k))).to(
+                "cuda", tdt))
+            Ys.append(torch.zeros(csr.nrows, k, dtype=torch.float64 if mixed else tdt, device="cuda"))
+            sv, mb, sx = (4, 2, 4) if mixed else (8, 1, 8)
+            nbr = (csr.nrows + r - 1) // r
+            total_bytes += (csr.nnz * sv + m.numberOfBlocks * (4 + r * mb) + 4 * (nbr + 1) +
+                            k * (csr.ncols * sx + 2 * csr.nrows * 8))
+            flops += 2 * csr.nnz * k
+        batch = S.Batch(mats, Xs, Ys, mixed=mixed)
+        nclasses, njobs = batch.info()
+        for _ in range(args.warmup):
+            batch.launch()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(args.steps):
+            batch.launch()
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / args.steps
+        lines.append({"precision": "mixed" if mixed else "f64", "ms_per_step": round(ms, 4),
+                      "gbs": round(total_bytes / (ms * 1e-3) / 1e9, 2),
+                      "gflops": round(flops / (ms * 1e-3) / 1e9, 2),
+                      "spmv_per_s": round(sum(k for _, k in work) / (ms * 1e-3), 1),
+                      "graph_classes": nclasses, "jobs": njobs,
+                      "r_chosen": {str(r): c for r, c in sorted(chosen.items())}})
+        del batch, mats, Xs, Ys
+        torch.cuda.empty_cache()
+    peak, peak_kind = load_peaks()
+    line = {"metric": "batched SpMM GB/s (algorithmic bytes, one CUDA graph)", "value": lines[0]["gbs"],
+            "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": lines[0]["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "batched", "matrices": len(work),
+                       "desc": "banded, N log-uniform [2e3,2e5], bandwidth U[5,200], density 0.1, "
+                               "k in {1,4,8,16}, seed 3, r per matrix by the autotuner (model)",
+                       "nnz": int(sum(c.nnz for c, _ in work))},
+            "precisions": lines,
+            "roofline": {"bound": "hbm", "achieved": lines[0]["gbs"], "peak": peak, "unit": "GB/s",
+                         "frac": round(lines[0]["gbs"] / peak, 4), "peak_kind": peak_kind}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# serving workload: resident pool, Poisson arrivals, Zipf matrix choice
+# ---------------------------------------------------------------------------
+
+def serve_pool():
+    """Eight distinct matrices (power-law and 27-point stencil styles, N from
+    ~50K to ~2M); each is registered eight times, giving 64 resident
+    matrices."""
+    return [M.powerlaw(50_000, seed=21), M.stencil27(60), M.powerlaw(300_000, seed=22),
+            M.stencil27(80), M.powerlaw(1_000_000, seed=23), M.stencil27(100),
+            M.powerlaw(2_000_000, seed=24), M.stencil27(126)]
+
+
+def run_serve(args):
+    import torch
+
+    import spc5_b200 as S
+    torch.cuda.set_device(0)
+    distinct = serve_pool()
+    rates = [float(t) for t in args.rates.split(",")]
+    results = []
+    for mixed in (False, True):
+        dt = np.float32 if mixed else np.float64
+        tdt = torch.float32 if mixed else torch.float64
+        mats = []
+        for rep in range(8):
+            for csr in distinct:
+                m = S.csr_matrix(csr.rowptr, csr.colidx, csr.values.astype(dt), csr.ncols)
+                S.CSR_to_SPC5(m, S.FORMAT_OF_R[1 if csr.name.startswith("powerlaw") else 4])
+                mats.append((m, csr))
+        srv = S.Server(slots=args.slots, max_k=16, mixed=mixed)
+        ids = [srv.add_matrix(m) for m, _ in mats]
+        resident = srv.stats()["resident_bytes"]
+        xs = [torch.from_numpy(M.x_vector(csr.ncols, 500 + i, dt)).cuda() for i, csr in enumerate(distinct)]
+        depth = 32  # enough outstanding outputs per matrix that arrivals never wait
+        ybufs = [[torch.empty(csr.nrows, dtype=torch.float64, device="cuda") for _ in range(depth)]
+                 for _, csr in mats]
+        owner = [[None] * depth for _ in mats]
+        zipf_w = 1.0 / np.arange(1, len(mats) + 1) ** 1.1
+        zipf_w /= zipf_w.sum()
+        for rate in rates:
+            rng = np.random.default_rng(int(rate))
+            nreq = int(rate * args.serve_seconds)
+            arrivals = np.cumsum(rng.exponential(1.0 / rate, size=nreq))
+            choice = rng.choice(len(mats), size=nreq, p=zipf_w)
+            srv.stats(reset=True)
+            slot_ptr = [0] * len(mats)
+            t0 = time.perf_counter()
+            for t_arr, i in zip(arrivals, choice):
+                while time.perf_counter() - t0 < t_arr:
+                    pass
+                j = slot_ptr[i]
+                slot_ptr[i] = (j + 1) % depth
+                if owner[i][j] is not None:
+                    srv.wait(owner[i][j])
+                owner[i][j] = srv.submit(ids[i], xs[i % len(distinct)], ybufs[i][j])
+            srv.drain()
+            for row in owner:
+                for j in range(depth):
+                    row[j] = None
+            st = srv.stats(reset=True)
+            results.append({"precision": "mixed" if mixed else "f64", "offered_req_per_s": rate,
+                            "req_per_s": round(st["req_per_s"], 1), "p50_us": round(st["p50_us"], 1),
+                            "p99_us": round(st["p99_us"], 1), "mean_k": round(st["mean_k"], 2),
+                            "launches": st["launches"], "completed": st["completed"],
+                            "resident_gb": round(resident / 1e9, 2)})
+        srv.close()
+        del mats, ybufs, xs
+        torch.cuda.empty_cache()
+    best = max(r["req_per_s"] for r in results if r["precision"] == "f64")
+    line = {"metric": "served SpMV req/s and p50/p99 latency", "value": best, "unit": "req/s",
+            "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "serve", "resident_matrices": 64,
+                       "desc": "8 distinct power-law / 27-point stencil matrices (N 50K..2M), each "
+                               "registered 8 times; Poisson arrivals, Zipf(1.1) matrix choice, "
+                               f"coalescing up to k=16, {args.slots} slots",
+                       "seconds_per_rate": args.serve_seconds},
+            "serving": results}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["powerlaw", "stencil27", "poisson"], default="powerlaw")
+    ap.add_argument("--workload", choices=["powerlaw", "stencil27", "poisson", "batched", "serve"],
+                    default="powerlaw")
+    ap.add_argument("--batch-count", type=int, default=256)
+    ap.add_argument("--rates", default="5000,20000,50000", help="serving arrival rates (req/s)")
+    ap.add_argument("--serve-seconds", type=float, default=2.0)
+    ap.add_argument("--slots", type=int, default=4)
     ap.add_argument("--size", type=int, default=None,
                     help="smaller workload for profiling (rows for powerlaw, grid edge for stencil27)")
     ap.add_argument("--formats", default="1,2,4,8", help="comma list of r to run")
@@ -415,6 +581,10 @@ def main():
     FORMATS = tuple(int(t) for t in args.formats.split(","))
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batched":
+        return run_batched(args)
+    if args.workload == "serve":
+        return run_serve(args)
     return run_gpu(args)
 
 

@@ -193,6 +193,23 @@ SPC5CUDA_API spc5cuda_status spc5cuda_spmm(const spc5cuda_mat* mat, int k, const
 SPC5CUDA_API spc5cuda_status spc5cuda_spmm_mixed(const spc5cuda_mat* mat, int k, const float* X,
                                                  long ldx, double* Y, long ldy, void* stream);
 
+/* COO triplets -> CSR handle on the device, following COO_sorted_to_CSR /
+ * COO_unsorted_to_CSR (spc5.hpp:77-114): sorted == 0 sorts by (row, column)
+ * first.  Duplicate (row, column) entries are rejected (SPC5CUDA_ERR_INVALID):
+ * the beta conversion needs unique columns per row.  Synchronises stream. */
+SPC5CUDA_API spc5cuda_status spc5cuda_mat_create_coo(spc5cuda_mat** out, int value_type,
+                                                     int nrows, int ncols, long nnz,
+                                                     const int* rows, const int* cols,
+                                                     const void* values, int on_device, int sorted,
+                                                     void* stream);
+
+/* Converted matrix -> COO triplets in storage order (block by block, sub-row,
+ * column), the corrected core_SPC5_rVc_iterate (spc5.hpp:255-273; the
+ * reference reads the masks at the block-row index, line 263).  Device
+ * outputs of nnz entries each. */
+SPC5CUDA_API spc5cuda_status spc5cuda_decode_coo(const spc5cuda_mat* mat, int* rows, int* cols,
+                                                 void* values, void* stream);
+
 /* ------------------------------------------------------------------------
  * Format selection.
  * ---------------------------------------------------------------------- */

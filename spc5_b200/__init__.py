@@ -48,6 +48,7 @@ EXPORTED_SYMBOLS = [
     "spc5cuda_batch_info", "spc5cuda_batch_destroy", "spc5cuda_server_create",
     "spc5cuda_server_add_matrix", "spc5cuda_server_submit", "spc5cuda_server_wait",
     "spc5cuda_server_drain", "spc5cuda_server_get_stats", "spc5cuda_server_destroy",
+    "spc5cuda_mat_create_coo", "spc5cuda_decode_coo",
 ]
 
 TUNE_MODEL = 0
@@ -158,6 +159,10 @@ def _lib():
         lib.spc5cuda_server_get_stats.argtypes = [_P, C.POINTER(spc5cuda_server_stats), _I]
         lib.spc5cuda_server_destroy.restype = _I
         lib.spc5cuda_server_destroy.argtypes = [_P]
+        lib.spc5cuda_mat_create_coo.restype = _I
+        lib.spc5cuda_mat_create_coo.argtypes = [C.POINTER(_P), _I, _I, _I, _L, _P, _P, _P, _I, _I, _P]
+        lib.spc5cuda_decode_coo.restype = _I
+        lib.spc5cuda_decode_coo.argtypes = [_P, _P, _P, _P, _P]
         _LIB = lib
     return _LIB
 
@@ -299,6 +304,47 @@ def csr_matrix(rowptr, colidx, values, ncols: int, dtype=None, stream=None) -> S
                                           1 if on_device else 0, st), "spc5cuda_mat_create_csr")
     del keep
     return SPC5Mat(h)
+
+
+def coo_matrix(nrows: int, ncols: int, rows, cols, values, sorted: bool = False,
+               stream=None) -> SPC5Mat:
+    """A CSR ``SPC5Mat`` from COO triplets, built on the device
+    (COO_sorted_to_CSR / COO_unsorted_to_CSR, spc5.hpp:77-114).  Host numpy
+    arrays or CUDA tensors; int32 indices."""
+    import torch
+    on_device = isinstance(rows, torch.Tensor) and rows.is_cuda
+    if on_device:
+        vt = _value_type(np.float64 if values.dtype == torch.float64 else np.float32)
+        ptrs = (_dptr(rows, torch.int32, "rows"), _dptr(cols, torch.int32, "cols"), _dptr(values))
+        nnz = rows.numel()
+        keep = (rows, cols, values)
+    else:
+        r_ = np.ascontiguousarray(rows, dtype=np.int32)
+        c_ = np.ascontiguousarray(cols, dtype=np.int32)
+        v_ = np.ascontiguousarray(values)
+        vt = _value_type(v_.dtype)
+        ptrs = (_np_ptr(r_), _np_ptr(c_), _np_ptr(v_))
+        nnz = len(r_)
+        keep = (r_, c_, v_)
+    h = C.c_void_p()
+    _check(_lib().spc5cuda_mat_create_coo(C.byref(h), vt, int(nrows), int(ncols), nnz, *ptrs,
+                                          1 if on_device else 0, 1 if sorted else 0, _stream(stream)),
+           "spc5cuda_mat_create_coo")
+    del keep
+    return SPC5Mat(h)
+
+
+def decode_coo(mat: SPC5Mat, stream=None):
+    """(rows, cols, values) CUDA tensors of a converted matrix in storage order."""
+    import torch
+    inf = mat.info()
+    dt = torch.float64 if inf.value_type == F64 else torch.float32
+    rows = torch.empty(inf.nnz, dtype=torch.int32, device="cuda")
+    cols = torch.empty(inf.nnz, dtype=torch.int32, device="cuda")
+    vals = torch.empty(inf.nnz, dtype=dt, device="cuda")
+    _check(_lib().spc5cuda_decode_coo(mat.handle, C.c_void_p(rows.data_ptr()), C.c_void_p(cols.data_ptr()),
+                                      C.c_void_p(vals.data_ptr()), _stream(stream)), "decode_coo")
+    return rows, cols, vals
 
 
 def beta_matrix(r: int, nrows: int, ncols: int, rowsSize, headers, values, stream=None) -> SPC5Mat:
