@@ -173,7 +173,7 @@ SPC5CUDA_API spc5cuda_status spc5cuda_get_arrays(const spc5cuda_mat* mat, int* r
                                     unsigned char* headers, void* values, int to_host,
                                     void* stream);
 
-/* SPC5_Spmv (spc5.hpp:1064-1088): y += A x, device x (ncols) and y (nrows)
+/* SPC5_Spmv (spc5.hpp:1090-1118): y += A x, device x (ncols) and y (nrows)
  * of the handle's value type. */
 SPC5CUDA_API spc5cuda_status spc5cuda_spmv(const spc5cuda_mat* mat, const void* x, void* y, void* stream);
 

@@ -124,7 +124,7 @@ int ref_f64_convert(void* h, int r) { return convert<double>(static_cast<RefMat<
 void ref_f64_get(void* h, int* rowptr, unsigned char* headers, double* values) {
     get<double>(static_cast<RefMat<double>*>(h), rowptr, headers, values);
 }
-// SPC5_Spmv<double> -> core_SPC5_{r}rVc_Spmv_double (spc5.hpp:1064-1088)
+// SPC5_Spmv<double> -> core_SPC5_{r}rVc_Spmv_double (spc5.hpp:1090-1118)
 void ref_f64_spmv(void* h, const double* x, double* y) {
     SPC5_Spmv<double>(static_cast<RefMat<double>*>(h)->mat, x, y);
 }
@@ -146,7 +146,7 @@ int ref_f64_find_best(void* h, double* estimate) {
 }
 
 #ifdef _OPENMP
-// SPC5_split_omp (spc5.hpp:1307-1334) with an explicit thread count
+// SPC5_split_omp (spc5.hpp:1307-1336) with an explicit thread count
 int ref_f64_split(void* h, int nthreads) {
     auto* m = static_cast<RefMat<double>*>(h);
     switch (m->r) {
@@ -158,7 +158,7 @@ int ref_f64_split(void* h, int nthreads) {
     }
     return int(m->split.size());
 }
-// One SPC5_Spmv_omp call (spc5.hpp:1336-1367); requires ref_f64_split
+// One SPC5_Spmv_omp call (spc5.hpp:1338-1367); requires ref_f64_split
 void ref_f64_spmv_omp(void* h, const double* x, double* y) {
     auto* m = static_cast<RefMat<double>*>(h);
     SPC5_Spmv_omp<double>(m->mat, x, y, m->split);

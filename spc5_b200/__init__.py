@@ -382,7 +382,7 @@ def CSR_to_SPC5(mat: SPC5Mat, fmt: int, stream=None) -> None:
 
 
 def SPC5_Spmv(mat: SPC5Mat, x, y, stream=None) -> None:
-    """y += A x (SPC5_Spmv, spc5.hpp:1064-1088); x, y CUDA tensors of the
+    """y += A x (SPC5_Spmv, spc5.hpp:1090-1118); x, y CUDA tensors of the
     matrix's value type."""
     import torch
     dt = torch.float64 if mat.dtype == np.float64 else torch.float32
