@@ -118,6 +118,25 @@ SPC5CUDA_API spc5cuda_status spc5cuda_core_spmv_f32(int r, long nbRows, const in
                                        const unsigned char* headers, const float* values,
                                        const float* x, float* y, void* stream);
 
+/* FP64 drop-in that allocates nothing (no counterpart in the reference).
+ * For callers that may not allocate device memory during the call -- an
+ * application that fixes its memory budget at start-up, a real-time loop
+ * that must stay out of the allocator, or a host whose memory pool belongs
+ * to another framework.  Same arguments and result as
+ * spc5cuda_core_spmv_f64; the per-call scratch lives in one file-scope
+ * device array of ~4.5 MB that every GPU loading the library keeps until the
+ * process exits.  Limit: ceil(nbRows / r) <= 1,048,576 block-rows, else
+ * SPC5CUDA_ERR_INVALID.  The first call on a device looks up the array's
+ * address with that device current, so make it before any stream capture.
+ * All calls share the array: calls that overlap on the GPU (other streams or
+ * threads without ordering) race; order them on one stream. */
+SPC5CUDA_API spc5cuda_status spc5cuda_core_spmv_f64_noalloc(int r, long nbRows,
+                                                            const int* rowsSizes,
+                                                            const unsigned char* headers,
+                                                            const double* values,
+                                                            const double* x, double* y,
+                                                            void* stream);
+
 /* ------------------------------------------------------------------------
  * Matrix handle: the device-resident counterpart of SPC5Mat<T>
  * (spc5.hpp:44-62) plus the precomputed partition that replaces the OpenMP

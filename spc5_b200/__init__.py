@@ -48,7 +48,7 @@ EXPORTED_SYMBOLS = [
     "spc5cuda_batch_info", "spc5cuda_batch_destroy", "spc5cuda_server_create",
     "spc5cuda_server_add_matrix", "spc5cuda_server_submit", "spc5cuda_server_wait",
     "spc5cuda_server_drain", "spc5cuda_server_get_stats", "spc5cuda_server_destroy",
-    "spc5cuda_mat_create_coo", "spc5cuda_decode_coo",
+    "spc5cuda_mat_create_coo", "spc5cuda_decode_coo", "spc5cuda_core_spmv_f64_noalloc",
 ]
 
 TUNE_MODEL = 0
