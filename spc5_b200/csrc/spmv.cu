@@ -19,12 +19,21 @@
 // Work split (replaces the OpenMP ThreadInterval split, spc5.hpp:346-427):
 // every group gets one contiguous range of block-rows holding about
 // nblocks / groups blocks (gstart[], built on the device).  A group streams
-// its range in chunks of VS blocks: lane j loads the packed header of block
-// j of the chunk (consecutive records, one coalesced access), the group
-// scans the per-block value counts to get each block's value offset, and the
-// next chunk's headers and row ends are loaded before the current chunk is
-// processed.  Values and headers are read once (streaming loads, evict
-// first); x goes through L1/L2.
+// its range in windows of up to VS blocks:
+//   * lane j loads the packed header of block j of the window two windows
+//     ahead (consecutive records, one coalesced access);
+//   * one window ahead, the group scans the per-block value counts, packs
+//     each block's mask with the staging-buffer offsets of its sub-rows into
+//     one broadcast word, and copies the window's values into shared memory
+//     with 16-byte cp.async (double-buffered);
+//   * for the current window, every lane first issues its x loads for all
+//     blocks (x[col + c] where any sub-row has bit c; L1/L2-cached, so the
+//     loads of a whole window are in flight together), then runs the FMAs.
+// When a block-row ends, each lane stores its accumulators to a per-group
+// slot in shared memory; the slots of a window are reduced together at its
+// end, one lane per (block-row, sub-row), with the same tree.
+#include <climits>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -33,19 +42,10 @@ namespace spc5cuda {
 namespace {
 
 constexpr int SPMV_CTAS_PER_SM = 16;
-
-template <int VS>
-__device__ __forceinline__ unsigned group_mask(int lane) {
-    return (VS == 32 ? 0xffffffffu : ((1u << VS) - 1u)) << (lane & ~(VS - 1));
-}
+constexpr unsigned FULL = 0xffffffffu;
 
 // Streaming 32-bit load of header words (read once).
 __device__ __forceinline__ uint32_t ld_stream_u32(const uint32_t* p) { return __ldcs(p); }
-
-template <class V>
-__device__ __forceinline__ V ld_stream(const V* p) {
-    return __ldcs(p);
-}
 
 // Header of block b decoded from aligned 32-bit words (each word holds at
 // least one byte of the record, so none reads past the array).
@@ -76,13 +76,6 @@ __device__ __forceinline__ void cp_async16(uint32_t saddr, const void* gptr) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(gptr) : "memory");
 }
 
-// Asynchronous 4- or 8-byte global -> shared copy (cached in L1: x is reused).
-template <int BYTES>
-__device__ __forceinline__ void cp_async_small(uint32_t saddr, const void* gptr) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(saddr), "l"(gptr), "n"(BYTES)
-                 : "memory");
-}
-
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 
 // Waits until at most one committed group of this thread is still in flight.
@@ -92,60 +85,80 @@ __device__ __forceinline__ void cp_async_wait_prev() {
 
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-// Byte-wise population count of a 32-bit word (SWAR).
-__device__ __forceinline__ uint32_t popc_bytes(uint32_t w) {
-    w = w - ((w >> 1) & 0x55555555u);
-    w = (w & 0x33333333u) + ((w >> 2) & 0x33333333u);
-    return (w + (w >> 4)) & 0x0F0F0F0Fu;
-}
+// Mask words hold one field per sub-row: a byte (f64, VS = 8) or a half-word
+// (f32, VS = 16).  Fields<MB> does per-field arithmetic on whole words.
+template <int MB>
+struct Fields;
 
-// OR of the r masks of one block folded onto the VS lane bits.
-template <class LT, int R>
-__device__ __forceinline__ uint32_t lanes_of(const uint32_t (&mw)[Header<LT, R>::MASK_WORDS]) {
-    uint32_t w = 0;
-#pragma unroll
-    for (int q = 0; q < Header<LT, R>::MASK_WORDS; ++q) w |= mw[q];
-    if constexpr (Layout<LT>::MASK_BYTES == 1) {
+template <>
+struct Fields<1> {
+    static constexpr uint32_t REP = 0x01010101u;  // one in every field
+    static constexpr int BITS = 8;
+    static constexpr int PER_WORD = 4;
+    // population count of every byte (SWAR)
+    __device__ static __forceinline__ uint32_t popc(uint32_t w) {
+        w = w - ((w >> 1) & 0x55555555u);
+        w = (w & 0x33333333u) + ((w >> 2) & 0x33333333u);
+        return (w + (w >> 4)) & 0x0F0F0F0Fu;
+    }
+    // exclusive prefix of the fields (field k = sum of fields below k)
+    __device__ static __forceinline__ uint32_t prefix(uint32_t f) { return f * 0x01010100u; }
+    __device__ static __forceinline__ uint32_t sum(uint32_t f) { return (f * 0x01010101u) >> 24; }
+    __device__ static __forceinline__ uint32_t get(uint32_t q, int k) { return (q >> (8 * k)) & 0xFFu; }
+    // OR of the fields
+    __device__ static __forceinline__ uint32_t fold(uint32_t w) {
         w |= w >> 16;
         w |= w >> 8;
         return w & 0xFFu;
-    } else {
-        w |= w >> 16;
-        return w & 0xFFFFu;
     }
-}
+};
+
+template <>
+struct Fields<2> {
+    static constexpr uint32_t REP = 0x00010001u;
+    static constexpr int BITS = 16;
+    static constexpr int PER_WORD = 2;
+    __device__ static __forceinline__ uint32_t popc(uint32_t w) {
+        w = w - ((w >> 1) & 0x55555555u);
+        w = (w & 0x33333333u) + ((w >> 2) & 0x33333333u);
+        w = (w + (w >> 4)) & 0x0F0F0F0Fu;
+        return (w + (w >> 8)) & 0x001F001Fu;
+    }
+    __device__ static __forceinline__ uint32_t prefix(uint32_t f) { return f << 16; }
+    __device__ static __forceinline__ uint32_t sum(uint32_t f) { return (f + (f >> 16)) & 0xFFFFu; }
+    __device__ static __forceinline__ uint32_t get(uint32_t q, int k) { return (q >> (16 * k)) & 0xFFFFu; }
+    __device__ static __forceinline__ uint32_t fold(uint32_t w) { return (w | (w >> 16)) & 0xFFFFu; }
+};
 
 // Geometry of the kernel: a group of VS lanes (lane c = column c of every
 // block) owns one block-row stream; GPW groups per warp run in lockstep.
-template <class LT, int R, class V, class X, class A>
+template <class LT, int R, class V, class A>
 struct Geo {
     static constexpr int VS = Layout<LT>::VS;
+    static constexpr int MB = Layout<LT>::MASK_BYTES;
     static constexpr int THREADS = 128;
     static constexpr int GPW = 32 / VS;                      // groups per warp
     static constexpr int GPC = THREADS / VS;                 // groups per CTA
     static constexpr int EPU = 16 / int(sizeof(V));          // values per 16-byte unit
-    static constexpr int CAP = 1024 / int(sizeof(V));        // staged values per window
-    static constexpr int VBUF = CAP + 2 * EPU;               // + alignment slack
-    static constexpr int VBYTES = VBUF * int(sizeof(V));
-    static constexpr int XBYTES = VS * VS * int(sizeof(X));  // x of one window: [block][column]
-    static constexpr int BUF_BYTES = (VBYTES + XBYTES + 15) / 16 * 16;
-    static constexpr int RED_BYTES = R > 1 ? (R * VS * int(sizeof(A)) + 15) / 16 * 16 : 0;
-    static constexpr int GROUP_BYTES = 2 * BUF_BYTES + RED_BYTES;  // double-buffered windows
+    static constexpr int MW = Header<LT, R>::MASK_WORDS;
+    // masks of one block fit in 16 bits: one broadcast word carries the masks
+    // (low half) and the buffer offsets of the sub-rows (high half)
+    static constexpr bool PACKED = R * MB <= 2;
+    static constexpr int NW = PACKED ? 1 : 2 * MW;           // broadcast words per block
+    // staged values per window: a full window of 8-column f64 blocks at
+    // r = 1, else the densest window of a 27-point stencil (12 values per
+    // block) -- denser windows are shortened
+    static constexpr int CAP = (VS == 8) ? (R == 1 ? 64 : 96) : 256;
+    static constexpr int VBUF = ((CAP + 2 * EPU) * int(sizeof(V)) + 15) / 16 * 16;
+    // flushed block-rows per reduction batch: MAXS * R = VS items, one per lane
+    static constexpr int MAXS = VS / R > 0 ? VS / R : 1;
+    static constexpr int SLOT_BYTES = MAXS * R * VS * int(sizeof(A));
+    static constexpr int GROUP_BYTES = 2 * VBUF + SLOT_BYTES;
     static constexpr int SMEM = GPC * GROUP_BYTES;
-    static constexpr int MW = Header<LT, R>::MASK_WORDS;
-    static constexpr int PW = (R + 3) / 4;                   // packed sub-row prefixes
     static_assert(CAP >= VS * R, "a block must fit one window");
-};
-
-// One window of a group: lane j describes block j of the window (j < n).
-template <class LT, int R>
-struct Win {
-    static constexpr int MW = Header<LT, R>::MASK_WORDS;
-    static constexpr int PW = (R + 3) / 4;
-    uint32_t mw[MW];
-    uint32_t pre[PW];  // exclusive prefix of the sub-row value counts, one byte per sub-row
-    int voff;          // staging-buffer index of the block's first value
-    int n;             // blocks in the window (group-uniform)
+    static_assert(CAP + 2 * EPU + (R - 1) * VS + VS <= (MB == 1 ? 256 : 65536),
+                  "buffer offsets must fit one mask field");
+    static_assert(MAXS * R == VS, "one reduction item per lane");
 };
 
 // Headers of up to VS blocks starting at block p: lane j holds block p + j.
@@ -166,29 +179,40 @@ __device__ __forceinline__ void load_raw(Raw<LT, R>& rw, const uint8_t* __restri
     if (rw.ok) rw.col = load_header_stream<LT, R>(headers, long(p + j), rw.mw);
 }
 
+// One staged window of a group: lane j describes block j (j < n).
+template <int NW>
+struct Win {
+    uint32_t w[NW];  // broadcast words: masks and buffer offsets of the sub-rows
+    int col;
+    int n;       // blocks in the window (group-uniform)
+    int wstart;  // first block of the window (group-uniform)
+};
+
 template <class LT, int R, class V, class X, class A, class Y>
 __global__ void __launch_bounds__(128)
     k_spmv(int nrows, const int* __restrict__ brptr, const uint8_t* __restrict__ headers,
            const V* __restrict__ values, const int* __restrict__ valptr,
            const int* __restrict__ gstart, int ngroups, const X* __restrict__ x,
            Y* __restrict__ y) {
-    using G = Geo<LT, R, V, X, A>;
-    constexpr int VS = G::VS, MW = G::MW, PW = G::PW;
-    constexpr int MB = Layout<LT>::MASK_BYTES;
+    using G = Geo<LT, R, V, A>;
+    using F = Fields<G::MB>;
+    constexpr int VS = G::VS, MW = G::MW, NW = G::NW, PW = F::PER_WORD;
     constexpr bool Y_ATOMIC = sizeof(Y) == 8;  // red.add.f64 is y + s rounded once
-    constexpr unsigned FULL = 0xffffffffu;
-    constexpr unsigned VSMASK = (VS == 32) ? FULL : ((1u << VS) - 1u);
+    constexpr uint32_t VSMASK = (1u << VS) - 1u;
+    // keep the broadcast words of a window in registers between the x pass
+    // and the FMA pass when they are few, else shuffle them again
+    constexpr bool KEEP = NW * VS <= 8;
     extern __shared__ __align__(16) unsigned char smem[];
 
     const int lane = threadIdx.x & 31;
     const int c = lane & (VS - 1);
-    const int gbase_lane = lane & ~(VS - 1);
+    const int gshift = lane & ~(VS - 1);  // bit offset of this group in warp bitmaps
     const uint32_t below = (1u << c) - 1u;
     const int gi = threadIdx.x / VS;
     const int group = blockIdx.x * G::GPC + gi;
-    const uint32_t sgroup = uint32_t(__cvta_generic_to_shared(smem)) + uint32_t(gi * G::GROUP_BYTES);
-    unsigned char* pgroup = smem + gi * G::GROUP_BYTES;
-    A* red = reinterpret_cast<A*>(pgroup + 2 * G::BUF_BYTES);
+    unsigned char* gbase = smem + gi * G::GROUP_BYTES;
+    const uint32_t sgbase = uint32_t(__cvta_generic_to_shared(gbase));
+    A* slots = reinterpret_cast<A*>(gbase + 2 * G::VBUF);
 
     int r_begin = 0, r_end = 0;
     if (group < ngroups) {
@@ -201,79 +225,98 @@ __global__ void __launch_bounds__(128)
     int p = has ? __ldg(brptr + r_begin) : 0;  // first block of the next window to stage
     int v_next = has ? __ldg(valptr + r_begin) : 0;
 
-    // row bookkeeping: current block-row row = rbase + k, rend = its end block
+    // Row bookkeeping (group-uniform except ends / ends_nxt): block-row `row`
+    // is the next to flush; lane c holds the end (exclusive block index) of
+    // block-rows rbase + c (ends) and rbase + VS + c (ends_nxt); row = rbase + k.
     int row = r_begin, rbase = r_begin, k = 0;
-    int ends = (has && rbase + 1 + c <= r_end) ? __ldg(brptr + rbase + 1 + c) : 0x7fffffff;
-    int ends_nxt = (has && rbase + 1 + VS + c <= r_end) ? __ldg(brptr + rbase + 1 + VS + c) : 0x7fffffff;
+    int ends = (has && rbase + c < r_end) ? __ldg(brptr + rbase + 1 + c) : INT_MAX;
+    int ends_nxt = (has && rbase + VS + c < r_end) ? __ldg(brptr + rbase + 1 + VS + c) : INT_MAX;
     int rend = __shfl_sync(FULL, ends, 0, VS);
-    Y ycur = Y(0);
-    if (!Y_ATOMIC && has && c < R && row * R + c < nrows) ycur = y[row * R + c];
+    int ns = 0;    // slots holding flushed block-rows
+    int srow = 0;  // block-row of slot 0
 
     A acc[R];
 #pragma unroll
     for (int i = 0; i < R; ++i) acc[i] = A(0);
 
-    // Flush every group whose current block-row ends at block position pos,
-    // repeating for empty block-rows; warp-uniform control flow.  The row sum
-    // is the _mm512_reduce_add tree over the VS lane accumulators: distance
-    // VS/2 first, then VS/4, ..., 1.
-    auto flush_while = [&](bool active, int pos) {
-        for (;;) {
-            const bool need = active && row < r_end && pos == rend;
-            if (!__any_sync(FULL, need)) break;
-            A s = A(0);
-            if constexpr (R == 1) {
-                s = acc[0];
+    // Reduce the flushed block-rows held in the slots: lane t takes item t =
+    // (slot t / R, sub-row t % R) and sums its VS lane values with the
+    // _mm512_reduce_add tree (distance VS/2 first, then VS/4, ..., 1).
+    auto reduce_batch = [&](bool doit) {
+        __syncwarp();
+        if (doit && c < ns * R) {
+            A a[VS];
+            const A* sp = slots + c * VS;
+            if constexpr (sizeof(A) == 8) {
 #pragma unroll
-                for (int d = VS / 2; d >= 1; d >>= 1) s += __shfl_xor_sync(FULL, s, d, VS);
+                for (int e = 0; e < VS; e += 2) {
+                    const double2 t = *reinterpret_cast<const double2*>(sp + e);
+                    a[e] = A(t.x);
+                    a[e + 1] = A(t.y);
+                }
             } else {
-                if (need) {
 #pragma unroll
-                    for (int i = 0; i < R; ++i) red[i * VS + c] = acc[i];
+                for (int e = 0; e < VS; e += 4) {
+                    const float4 t = *reinterpret_cast<const float4*>(sp + e);
+                    a[e] = A(t.x);
+                    a[e + 1] = A(t.y);
+                    a[e + 2] = A(t.z);
+                    a[e + 3] = A(t.w);
                 }
-                __syncwarp();
-                if (need && c < R) {
-                    A a[VS];
-#pragma unroll
-                    for (int e = 0; e < VS; ++e) a[e] = red[c * VS + e];
-#pragma unroll
-                    for (int d = VS / 2; d >= 1; d >>= 1) {
-#pragma unroll
-                        for (int e = 0; e < d; ++e) a[e] = a[e] + a[e + d];
-                    }
-                    s = a[0];
-                }
-                __syncwarp();
             }
-            if (need) {
-                const int yrow = row * R + c;
-                if (c < R && yrow < nrows) {
-                    if constexpr (Y_ATOMIC) atomicAdd(y + yrow, Y(s));
-                    else y[yrow] = ycur + Y(s);
-                }
 #pragma unroll
-                for (int i = 0; i < R; ++i) acc[i] = A(0);
+            for (int d = VS / 2; d >= 1; d >>= 1) {
+#pragma unroll
+                for (int e = 0; e < d; ++e) a[e] = a[e] + a[e + d];
+            }
+            const long yrow = long(srow + c / R) * R + (c % R);
+            if (yrow < nrows) {
+                if constexpr (Y_ATOMIC) atomicAdd(y + yrow, Y(a[0]));
+                else y[yrow] = y[yrow] + Y(a[0]);
+            }
+        }
+        if (doit) ns = 0;
+        __syncwarp();
+    };
+
+    // Flush every group whose current block-row ends at block b (the rows
+    // that end before block b is processed), repeating for empty block-rows;
+    // warp-uniform control flow.
+    auto flush_exact = [&](int b, bool active) {
+        for (;;) {
+            const bool fl = active && row < r_end && rend == b;
+            if (!__any_sync(FULL, fl)) break;
+            if (fl) {
+                if (ns == 0) srow = row;
+                A* sp = slots + ns * (R * VS) + c;
+#pragma unroll
+                for (int i = 0; i < R; ++i) {
+                    sp[i * VS] = acc[i];
+                    acc[i] = A(0);
+                }
+                ++ns;
                 ++row;
                 if (++k == VS) {
                     k = 0;
                     rbase += VS;
                     ends = ends_nxt;
-                    ends_nxt = (rbase + 1 + VS + c <= r_end) ? __ldg(brptr + rbase + 1 + VS + c) : 0x7fffffff;
-                }
-                if constexpr (!Y_ATOMIC) {
-                    const int ynext = row * R + c;
-                    if (c < R && row < r_end && ynext < nrows) ycur = y[ynext];
+                    ends_nxt = (rbase + VS + c < r_end) ? __ldg(brptr + rbase + 1 + VS + c) : INT_MAX;
                 }
             }
             rend = __shfl_sync(FULL, ends, k, VS);
+            if (__any_sync(FULL, ns == G::MAXS)) reduce_batch(ns == G::MAXS);
         }
     };
 
-    // ---- stage one window: headers rw (blocks p ...) -> win; values and x into buffer bi
-    auto stage = [&](const Raw<LT, R>& rw, Win<LT, R>& win, int bi) {
+    // ---- stage one window: headers rw (blocks p ...) -> win; values into buffer bi
+    auto stage = [&](const Raw<LT, R>& rw, Win<NW>& win, int bi) {
+        uint32_t cnt[MW];
         int tot = 0;
 #pragma unroll
-        for (int q = 0; q < MW; ++q) tot += __popc(rw.mw[q]);
+        for (int q = 0; q < MW; ++q) {
+            cnt[q] = F::popc(rw.mw[q]);
+            tot += int(F::sum(cnt[q]));
+        }
         if (!rw.ok) tot = 0;
         int incl = tot;
 #pragma unroll
@@ -281,132 +324,143 @@ __global__ void __launch_bounds__(128)
             const int t = __shfl_up_sync(FULL, incl, d, VS);
             if (c >= d) incl += t;
         }
-        const int n = __popc((__ballot_sync(FULL, rw.ok && incl <= G::CAP) >> gbase_lane) & VSMASK);
+        const int n = __popc((__ballot_sync(FULL, rw.ok && incl <= G::CAP) >> gshift) & VSMASK);
         const int tv = __shfl_sync(FULL, incl, (n > 0 ? n : 1) - 1, VS);
         const int s0 = v_next & ~(G::EPU - 1);
         const int shift = v_next - s0;
+        const uint32_t voff = uint32_t(shift + incl - tot);  // buffer index of the block's first value
         win.n = n;
+        win.wstart = p;
+        win.col = rw.col;
+        if constexpr (G::PACKED) {
+            const uint32_t base = (voff * F::REP + F::prefix(cnt[0])) & 0xFFFFu;
+            win.w[0] = rw.mw[0] | (base << 16);
+        } else {
+            uint32_t carry = 0;
 #pragma unroll
-        for (int q = 0; q < MW; ++q) win.mw[q] = rw.mw[q];
-        win.voff = shift + incl - tot;
-        {
-            uint32_t run = 0;
-#pragma unroll
-            for (int q = 0; q < PW; ++q) win.pre[q] = 0u;
-#pragma unroll
-            for (int i = 0; i < R; ++i) {
-                win.pre[i >> 2] |= run << ((i & 3) * 8);
-                run += __popc(mask_of<LT, R>(rw.mw, i));
+            for (int q = 0; q < MW; ++q) {
+                win.w[q] = rw.mw[q];
+                win.w[MW + q] = (voff + carry) * F::REP + F::prefix(cnt[q]);
+                carry += F::sum(cnt[q]);
             }
         }
-        const uint32_t vb = sgroup + uint32_t(bi * G::BUF_BYTES);
         if (n > 0) {
+            const uint32_t vb = sgbase + uint32_t(bi * G::VBUF);
             const int units = (shift + tv + G::EPU - 1) / G::EPU;
             const V* src = values + s0;
             for (int u = c; u < units; u += VS) cp_async16(vb + uint32_t(u) * 16u, src + u * G::EPU);
-        }
-        // x: lane c copies column c of every block that holds a value there
-        {
-            const uint32_t lor = lanes_of<LT, R>(rw.mw);
-            const uint32_t xb = vb + uint32_t(G::VBYTES) + uint32_t(c) * uint32_t(sizeof(X));
-#pragma unroll
-            for (int j = 0; j < VS; ++j) {
-                const int cj = __shfl_sync(FULL, rw.col, j, VS);
-                const uint32_t lj = __shfl_sync(FULL, lor, j, VS);
-                if (j < n && ((lj >> c) & 1u))
-                    cp_async_small<int(sizeof(X))>(xb + uint32_t(j * VS) * uint32_t(sizeof(X)), x + (cj + c));
-            }
         }
         cp_async_commit();
         v_next += (n > 0) ? tv : 0;
         p += n;
     };
 
+    // masks (q-th word) and buffer offsets (q-th word) of a broadcast block
+    auto mask_word = [&](const uint32_t (&w)[NW], int q) -> uint32_t {
+        if constexpr (G::PACKED) return w[0] & 0xFFFFu;
+        else return w[q];
+    };
+    auto base_word = [&](const uint32_t (&w)[NW], int q) -> uint32_t {
+        if constexpr (G::PACKED) return w[0] >> 16;
+        else return w[MW + q];
+    };
+
     // ---- prologue: stage window 0, load the headers of window 1
     Raw<LT, R> raw;
     load_raw<LT, R>(raw, headers, p, b_stop, c);
-    Win<LT, R> cur;
-    int wstart = p;  // first block of the current window
+    Win<NW> cur;
     stage(raw, cur, 0);
     load_raw<LT, R>(raw, headers, p, b_stop, c);
     int bi = 0;
 
     while (__any_sync(FULL, cur.n > 0)) {
-        Win<LT, R> nxt;
-        const int nstart = p;
+        // ---- x pass: every lane loads x[col + c] of every block of the window
+        // in which some sub-row has bit c
+        X xv[VS];
+        uint32_t keep[KEEP ? VS : 1][NW];
+#pragma unroll
+        for (int j = 0; j < VS; ++j) {
+            if (!__any_sync(FULL, j < cur.n)) break;
+            const int cj = __shfl_sync(FULL, cur.col, j, VS);
+            uint32_t wj[NW];
+#pragma unroll
+            for (int q = 0; q < NW; ++q) wj[q] = __shfl_sync(FULL, cur.w[q], j, VS);
+            uint32_t lanes = 0;
+#pragma unroll
+            for (int q = 0; q < MW; ++q) lanes |= F::fold(mask_word(wj, q));
+            xv[j] = X(0);
+            if (j < cur.n && ((lanes >> c) & 1u)) xv[j] = __ldg(x + (cj + c));
+            if constexpr (KEEP) {
+#pragma unroll
+                for (int q = 0; q < NW; ++q) keep[j][q] = wj[q];
+            }
+        }
+
+        // ---- stage the next window, load the headers of the one after it
+        Win<NW> nxt;
         stage(raw, nxt, bi ^ 1);
         load_raw<LT, R>(raw, headers, p, b_stop, c);
 
-        // block positions of this window where a block-row of some group ends
-        // (known row ends: ends of rows rbase+1 .. rbase+VS, ends_nxt beyond);
-        // positions past the last known end are checked individually.
+        // ---- block positions of this window where a block-row of some group
+        // may end (known ends of rows row .. rbase + 2 VS - 1; past the last
+        // known end every position is checked)
         uint32_t rmask;
         {
-            const int rel = ends - wstart;
-            uint32_t mine = (rel >= 0 && rel < VS) ? (1u << rel) : 0u;
+            uint32_t mine = 0;
+            const int rel = ends - cur.wstart;
+            if (c >= k && rel >= 0 && rel < cur.n) mine |= 1u << rel;
+            const int rel2 = ends_nxt - cur.wstart;
+            if (rel2 >= 0 && rel2 < cur.n) mine |= 1u << rel2;
             const int last = __shfl_sync(FULL, ends_nxt, VS - 1, VS);
-            const int lrel = last - wstart;
-            if (c == 0 && lrel < VS) mine |= VSMASK << (lrel < 0 ? 0 : lrel);
-            const int rel2 = ends_nxt - wstart;
-            if (rel2 >= 0 && rel2 < VS) mine |= 1u << rel2;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) mine |= __shfl_xor_sync(FULL, mine, d);
-            rmask = mine;
+            const int lrel = last - cur.wstart;
+            if (c == 0 && lrel < cur.n) mine |= VSMASK << (lrel < 0 ? 0 : lrel);
+            rmask = __reduce_or_sync(FULL, mine) & VSMASK;
         }
         cp_async_wait_prev();
         __syncwarp();
 
-        const V* vbuf = reinterpret_cast<const V*>(pgroup + bi * G::BUF_BYTES);
-        const X* xbuf = reinterpret_cast<const X*>(pgroup + bi * G::BUF_BYTES + G::VBYTES);
+        // ---- FMA pass
+        const V* vbuf = reinterpret_cast<const V*>(gbase + bi * G::VBUF);
 #pragma unroll
         for (int j = 0; j < VS; ++j) {
             if (!__any_sync(FULL, j < cur.n)) break;
             const bool act = j < cur.n;
-            uint32_t bm[MW];
+            if ((rmask >> j) & 1u) flush_exact(cur.wstart + j, act);
+            uint32_t wj[NW];
+            if constexpr (KEEP) {
 #pragma unroll
-            for (int q = 0; q < MW; ++q) bm[q] = __shfl_sync(FULL, cur.mw[q], j, VS);
-            uint32_t bp[PW];
+                for (int q = 0; q < NW; ++q) wj[q] = keep[j][q];
+            } else {
 #pragma unroll
-            for (int q = 0; q < PW; ++q) bp[q] = __shfl_sync(FULL, cur.pre[q], j, VS);
-            const int voff = __shfl_sync(FULL, cur.voff, j, VS);
-            if ((rmask >> j) & 1u) flush_while(act, wstart + j);
+                for (int q = 0; q < NW; ++q) wj[q] = __shfl_sync(FULL, cur.w[q], j, VS);
+            }
             if (act) {
-                const A xv = A(xbuf[j * VS + c]);
-                if constexpr (MB == 1 && R >= 2) {
+                const A xa = A(xv[j]);
 #pragma unroll
-                    for (int q = 0; q < MW; ++q) {
-                        const uint32_t Q = bp[q] + popc_bytes(bm[q] & (below * 0x01010101u));
+                for (int q = 0; q < MW; ++q) {
+                    const uint32_t m = mask_word(wj, q);
+                    uint32_t qoff;
+                    if constexpr (R == 1) qoff = base_word(wj, q) + uint32_t(__popc(m & below));
+                    else qoff = base_word(wj, q) + F::popc(m & (below * F::REP));
 #pragma unroll
-                        for (int ii = 0; ii < 4; ++ii) {
-                            const int i = q * 4 + ii;
-                            if (i < R && ((bm[q] >> (ii * 8 + c)) & 1u))
-                                acc[i] = fma(A(vbuf[voff + int((Q >> (ii * 8)) & 0xFFu)]), xv, acc[i]);
-                        }
-                    }
-                } else {
-#pragma unroll
-                    for (int i = 0; i < R; ++i) {
-                        const uint32_t m = mask_of<LT, R>(bm, i);
-                        if ((m >> c) & 1u) {
-                            const int idx = voff + int((bp[i >> 2] >> ((i & 3) * 8)) & 0xFFu) + __popc(m & below);
-                            acc[i] = fma(A(vbuf[idx]), xv, acc[i]);
-                        }
+                    for (int f = 0; f < PW; ++f) {
+                        const int i = q * PW + f;
+                        if (i < R && ((m >> (f * F::BITS + c)) & 1u))
+                            acc[i] = fma(A(vbuf[F::get(qoff, f)]), xa, acc[i]);
                     }
                 }
             }
         }
+        // the block-rows flushed in this window
+        if (__any_sync(FULL, ns > 0)) reduce_batch(ns > 0);
         __syncwarp();
         cur = nxt;
-        wstart = nstart;
         bi ^= 1;
     }
     cp_async_wait_all();
     // the last block-row of every range and any empty block-rows after it
-    for (;;) {
-        const bool need = row < r_end;
-        if (!__any_sync(FULL, need)) break;
-        flush_while(need, need ? rend : -1);
-    }
+    flush_exact(b_stop, has);
+    if (__any_sync(FULL, ns > 0)) reduce_batch(ns > 0);
 }
 
 // gstart[g] = first block-row whose first block lies in group g's share
@@ -440,7 +494,7 @@ void launch_impl(const BetaView& m, const X* x, Y* y, cudaStream_t s) {
     const V* vals = static_cast<const V*>(m.values);
 #define SPC5_LAUNCH(R_)                                                                          \
     {                                                                                            \
-        using G = Geo<LT, R_, V, X, A>;                                                          \
+        using G = Geo<LT, R_, V, A>;                                                          \
         const int ctas = (m.ngroups + G::GPC - 1) / G::GPC;                                      \
         auto kern = k_spmv<LT, R_, V, X, A, Y>;                                                  \
         set_smem(kern, G::SMEM);                                                                 \
@@ -467,7 +521,7 @@ int occupancy(int r) {
     int n = 0;
 #define SPC5_OCC(R_)                                                                             \
     {                                                                                            \
-        using G = Geo<LT, R_, V, X, A>;                                                          \
+        using G = Geo<LT, R_, V, A>;                                                          \
         auto kern = k_spmv<LT, R_, V, X, A, Y>;                                                  \
         set_smem(kern, G::SMEM);                                                                 \
         SPC5_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, G::THREADS, G::SMEM)); \
@@ -489,7 +543,7 @@ namespace {
 
 template <class LT, class V>
 int groups_per_cta(int) {
-    return Geo<LT, 1, V, V, V>::GPC;
+    return Geo<LT, 1, V, V>::GPC;
 }
 
 }  // namespace
