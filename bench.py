@@ -254,6 +254,7 @@ def run_gpu(args):
     for r in FORMATS:
         m = S.csr_matrix(csr.rowptr, csr.colidx, csr.values, csr.ncols)
         S.CSR_to_SPC5(m, S.FORMAT_OF_R[r])
+        select_kernel(m, args.kernel)
         mats.append((r, m))
         bytes_of[r] = spmv_bytes(csr.nnz, m.numberOfBlocks, r, csr.nrows, csr.ncols)
     step_bytes = sum(bytes_of.values())
@@ -330,6 +331,7 @@ def run_gpu(args):
         for r, m64 in mats:
             m32 = S.csr_matrix(csr.rowptr, csr.colidx, csr.values, csr.ncols, dtype=np.float32)
             S.CSR_to_SPC5(m32, S.FORMAT_OF_R[r])
+            select_kernel(m32, args.kernel)
             ym = torch.zeros_like(y)
             y_ref.zero_()
             S.SPC5_Spmv(m64, x, y_ref)
@@ -377,7 +379,9 @@ def run_gpu(args):
             "gflops": round(2 * csr.nnz * len(FORMATS) * args.steps * world / (ms * 1e-3) / 1e9, 2),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                         "traffic": args.traffic, "kernel": "k_spmv_groups (all r)"},
+                         "traffic": args.traffic,
+                         "kernel": ", ".join(sorted({KERNEL_NAME[m.kernel] for _, m in mats}))},
+            "kernels": {str(r): KERNEL_NAME[m.kernel] for r, m in mats},
             "e2e": {"value": round(e2e_value, 2), "unit": UNIT,
                     "h2d_bytes_per_step": int(x.numel() * 8 + y.numel() * 8),
                     "d2h_bytes_per_step": int(y.numel() * 8)},
@@ -555,6 +559,23 @@ def run_serve(args):
     return 0
 
 
+# spc5cuda_mat_kernel codes: SPC5CUDA_KERNEL_GROUPS = 1, SPC5CUDA_KERNEL_ROWS = 2
+KERNEL_NAME = {1: "k_spmv (group per block-row stream)", 2: "k_rows (thread per sub-row)",
+               0: "unconverted"}
+
+
+def select_kernel(m, which):
+    """Apply --kernel to a converted handle."""
+    import spc5_b200 as S
+    if which == "groups":
+        m.set_kernel(S.KERNEL_GROUPS)
+    elif which == "rows":
+        try:
+            m.set_kernel(S.KERNEL_ROWS)
+        except S.SPC5Error:
+            m.set_kernel(S.KERNEL_AUTO)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -572,6 +593,8 @@ def main():
     ap.add_argument("--formats", default="1,2,4,8", help="comma list of r to run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--kernel", choices=["auto", "groups", "rows"], default="auto",
+                    help="SpMV kernel (rows falls back to auto where a block-row does not fit)")
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu dram bytes per launch of the dominant kernel, if captured")
     args = ap.parse_args()

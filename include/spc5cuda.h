@@ -176,6 +176,23 @@ SPC5CUDA_API spc5cuda_status spc5cuda_mat_create_beta(spc5cuda_mat** out, int va
 SPC5CUDA_API spc5cuda_status spc5cuda_mat_destroy(spc5cuda_mat* mat);
 SPC5CUDA_API spc5cuda_status spc5cuda_mat_info(const spc5cuda_mat* mat, spc5cuda_info* out);
 
+/* SpMV kernel selection (no counterpart in the reference, which has one
+ * kernel per r and instruction set).  Both kernels give the same bits.
+ *   AUTO   -- for r <= 4, the thread-per-sub-row kernel when every
+ *             block-row fits its per-warp staging buffers (stencils, Poisson,
+ *             banded); otherwise the group kernel (one group of VS lanes per
+ *             block-row stream);
+ *   GROUPS -- always the group kernel;
+ *   ROWS   -- the thread-per-sub-row kernel; SPC5CUDA_ERR_UNSUPPORTED on a
+ *             converted matrix with a block-row that does not fit.
+ * spc5cuda_mat_kernel reports the kernel SpMV uses now (GROUPS or ROWS; AUTO
+ * before conversion). */
+#define SPC5CUDA_KERNEL_AUTO 0
+#define SPC5CUDA_KERNEL_GROUPS 1
+#define SPC5CUDA_KERNEL_ROWS 2
+SPC5CUDA_API spc5cuda_status spc5cuda_mat_set_kernel(spc5cuda_mat* mat, int kernel);
+SPC5CUDA_API spc5cuda_status spc5cuda_mat_kernel(const spc5cuda_mat* mat, int* kernel);
+
 /* SPC5_{r}rVc_block_count (spc5.hpp:510-513, 635-638, 764-767, 890-893):
  * number of blocks the conversion to r would produce.  CSR handles only.
  * Synchronises stream. */

@@ -49,10 +49,16 @@ EXPORTED_SYMBOLS = [
     "spc5cuda_server_add_matrix", "spc5cuda_server_submit", "spc5cuda_server_wait",
     "spc5cuda_server_drain", "spc5cuda_server_get_stats", "spc5cuda_server_destroy",
     "spc5cuda_mat_create_coo", "spc5cuda_decode_coo", "spc5cuda_core_spmv_f64_noalloc",
+    "spc5cuda_mat_set_kernel", "spc5cuda_mat_kernel",
 ]
 
 TUNE_MODEL = 0
 TUNE_MEASURE = 1
+
+# SpMV kernel selection (spc5cuda_mat_set_kernel)
+KERNEL_AUTO = 0
+KERNEL_GROUPS = 1
+KERNEL_ROWS = 2
 
 
 class SPC5Error(RuntimeError):
@@ -120,6 +126,10 @@ def _lib():
         lib.spc5cuda_mat_destroy.argtypes = [_P]
         lib.spc5cuda_mat_info.restype = _I
         lib.spc5cuda_mat_info.argtypes = [_P, C.POINTER(spc5cuda_info)]
+        lib.spc5cuda_mat_set_kernel.restype = _I
+        lib.spc5cuda_mat_set_kernel.argtypes = [_P, _I]
+        lib.spc5cuda_mat_kernel.restype = _I
+        lib.spc5cuda_mat_kernel.argtypes = [_P, C.POINTER(_I)]
         lib.spc5cuda_block_count.restype = _I
         lib.spc5cuda_block_count.argtypes = [_P, _I, C.POINTER(_L), _P]
         lib.spc5cuda_convert.restype = _I
@@ -231,6 +241,17 @@ class SPC5Mat:
         inf = spc5cuda_info()
         _check(_lib().spc5cuda_mat_info(self._h, C.byref(inf)), "spc5cuda_mat_info")
         return inf
+
+    def set_kernel(self, kernel: int) -> None:
+        """Select the SpMV kernel: KERNEL_AUTO, KERNEL_GROUPS or KERNEL_ROWS."""
+        _check(_lib().spc5cuda_mat_set_kernel(self._h, int(kernel)), "spc5cuda_mat_set_kernel")
+
+    @property
+    def kernel(self) -> int:
+        """The SpMV kernel in use: KERNEL_GROUPS or KERNEL_ROWS (KERNEL_AUTO before conversion)."""
+        k = C.c_int(0)
+        _check(_lib().spc5cuda_mat_kernel(self._h, C.byref(k)), "spc5cuda_mat_kernel")
+        return k.value
 
     @property
     def format(self) -> int:

@@ -267,6 +267,26 @@ spc5cuda_status spc5cuda_mat_info(const spc5cuda_mat* m, spc5cuda_info* out) {
     });
 }
 
+spc5cuda_status spc5cuda_mat_set_kernel(spc5cuda_mat* m, int kernel) {
+    return guarded([&] {
+        require(m, SPC5CUDA_ERR_INVALID, "null");
+        require(kernel == SPC5CUDA_KERNEL_AUTO || kernel == SPC5CUDA_KERNEL_GROUPS ||
+                    kernel == SPC5CUDA_KERNEL_ROWS,
+                SPC5CUDA_ERR_INVALID, "unknown kernel");
+        if (kernel == SPC5CUDA_KERNEL_ROWS && m->r != 0)
+            require(m->rows_ok, SPC5CUDA_ERR_UNSUPPORTED, "a block-row exceeds the row kernel's buffers");
+        m->kernel = kernel;
+    });
+}
+
+spc5cuda_status spc5cuda_mat_kernel(const spc5cuda_mat* m, int* kernel) {
+    return guarded([&] {
+        require(m && kernel, SPC5CUDA_ERR_INVALID, "null");
+        if (m->r == 0) *kernel = SPC5CUDA_KERNEL_AUTO;
+        else *kernel = m->use_rows() ? SPC5CUDA_KERNEL_ROWS : SPC5CUDA_KERNEL_GROUPS;
+    });
+}
+
 spc5cuda_status spc5cuda_block_count(const spc5cuda_mat* m, int r, long* nblocks, void* stream) {
     return guarded([&] {
         require(m && nblocks, SPC5CUDA_ERR_INVALID, "null");

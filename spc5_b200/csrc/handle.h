@@ -130,6 +130,10 @@ struct spc5cuda_mat {
     Owned valptr;   // ceil(nrows/r)+1 value offsets (not in the reference format)
     Owned gstart;   // ngroups+1 block-row starts of the per-group ranges
     int ngroups = 0;
+    Owned wstart;   // nwarps+1 block-row starts of the thread-per-sub-row kernel's warps
+    int nwarps = 0;
+    int kernel = SPC5CUDA_KERNEL_AUTO;  // SpMV kernel choice (spc5cuda_mat_set_kernel)
+    bool rows_ok = false;               // every block-row fits the row kernel's buffers
 
     int nbr() const { return r ? spc5cuda::div_up(nrows, r) : 0; }
     BetaView view() const {
@@ -143,17 +147,44 @@ struct spc5cuda_mat {
         v.valptr = valptr.as<int>();
         v.gstart = gstart.as<int>();
         v.ngroups = ngroups;
+        if (use_rows()) {
+            v.wstart = wstart.as<int>();
+            v.nwarps = nwarps;
+        }
         return v;
+    }
+    // The thread-per-sub-row kernel runs when every block-row fits its
+    // staging buffers: on request, or by default for r <= 4 (at r = 8 every
+    // block costs eight lanes a header decode each, and the group kernel is
+    // faster on the B200).
+    bool use_rows() const {
+        if (!rows_ok || nwarps <= 0) return false;
+        if (kernel == SPC5CUDA_KERNEL_ROWS) return true;
+        return kernel == SPC5CUDA_KERNEL_AUTO && r <= 4;
     }
     long device_bytes() const {
         return long(rowptr.bytes + colidx.bytes + values.bytes + brptr.bytes + headers.bytes +
-                    valptr.bytes + gstart.bytes);
+                    valptr.bytes + gstart.bytes + wstart.bytes);
     }
     // The per-group block-row ranges for the current device.
+    // The per-group block-row ranges for the current device, and the per-warp
+    // ranges of the thread-per-sub-row kernel when every block-row fits it.
     void build_partition(cudaStream_t s) {
-        ngroups = spc5cuda::spmv_groups(spc5cuda::vs_of(value_type), r);
+        const int vs = spc5cuda::vs_of(value_type);
+        ngroups = spc5cuda::spmv_groups(vs, r);
         gstart.alloc(sizeof(int) * size_t(ngroups + 1));
         spc5cuda::launch_partition(nbr(), brptr.as<int>(), ngroups, gstart.as<int>(), s);
+        int max_blocks = 0, max_values = 0;
+        spc5cuda::blockrow_max(nbr(), brptr.as<int>(), valptr.as<int>(), &max_blocks, &max_values, s);
+        rows_ok = spc5cuda::rows_fit(vs, r, max_blocks, max_values);
+        if (rows_ok) {
+            nwarps = spc5cuda::rows_warps(vs, r);
+            wstart.alloc(sizeof(int) * size_t(nwarps + 1));
+            spc5cuda::launch_partition(nbr(), brptr.as<int>(), nwarps, wstart.as<int>(), s);
+        } else {
+            nwarps = 0;
+            wstart.release();
+        }
     }
 };
 

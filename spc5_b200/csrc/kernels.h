@@ -38,15 +38,19 @@ void launch_blockrow_value_counts(int mask_bytes, int r, int nbr, const int* brp
 
 // ---- SpMV (spmv.cu) ------------------------------------------------------
 struct BetaView {
-    int r;
-    int nrows;
-    int nbr;            // ceil(nrows / r)
-    const int* brptr;   // nbr + 1 block offsets
-    const uint8_t* headers;
-    const void* values;
-    const int* valptr;  // nbr + 1 value offsets
-    const int* gstart;  // ngroups + 1 block-row starts of the group ranges
-    int ngroups;
+    int r = 0;
+    int nrows = 0;
+    int nbr = 0;                    // ceil(nrows / r)
+    const int* brptr = nullptr;     // nbr + 1 block offsets
+    const uint8_t* headers = nullptr;
+    const void* values = nullptr;
+    const int* valptr = nullptr;    // nbr + 1 value offsets
+    const int* gstart = nullptr;    // ngroups + 1 block-row starts of the group ranges
+    int ngroups = 0;
+    // thread-per-sub-row kernel (short block-rows): nwarps + 1 block-row
+    // starts of the per-warp ranges; null selects the group kernel
+    const int* wstart = nullptr;
+    int nwarps = 0;
 };
 
 // Number of VS-lane groups the SpMV kernels launch on the current device
@@ -57,6 +61,18 @@ int spmv_groups(int vs, int r);
 void launch_partition(int nbr, const int* brptr, int ngroups, int* gstart, cudaStream_t s);
 
 void launch_spmv_f64(const BetaView& m, const double* x, double* y, cudaStream_t s);
+
+// Thread-per-sub-row kernel (spmv_rows.cu): resident warps on this device,
+// whether block-rows of at most max_blocks blocks / max_values values fit its
+// staging buffers, and the largest block-row of a converted matrix
+// (synchronises s).
+int rows_warps(int vs, int r);
+bool rows_fit(int vs, int r, int max_blocks, int max_values);
+void blockrow_max(int nbr, const int* brptr, const int* valptr, int* max_blocks, int* max_values,
+                  cudaStream_t s);
+void launch_rows_f64(const BetaView& m, const double* x, double* y, cudaStream_t s);
+void launch_rows_f32(const BetaView& m, const float* x, float* y, cudaStream_t s);
+void launch_rows_mixed(const BetaView& m, const float* x, double* y, cudaStream_t s);
 void launch_spmv_f32(const BetaView& m, const float* x, float* y, cudaStream_t s);
 void launch_spmv_mixed(const BetaView& m, const float* x, double* y, cudaStream_t s);
 

@@ -571,15 +571,18 @@ void launch_partition(int nbr, const int* brptr, int ngroups, int* gstart, cudaS
 }
 
 void launch_spmv_f64(const BetaView& m, const double* x, double* y, cudaStream_t s) {
-    launch_impl<double, double, double, double, double>(m, x, y, s);
+    if (m.wstart) launch_rows_f64(m, x, y, s);
+    else launch_impl<double, double, double, double, double>(m, x, y, s);
 }
 
 void launch_spmv_f32(const BetaView& m, const float* x, float* y, cudaStream_t s) {
-    launch_impl<float, float, float, float, float>(m, x, y, s);
+    if (m.wstart) launch_rows_f32(m, x, y, s);
+    else launch_impl<float, float, float, float, float>(m, x, y, s);
 }
 
 void launch_spmv_mixed(const BetaView& m, const float* x, double* y, cudaStream_t s) {
-    launch_impl<float, float, float, double, double>(m, x, y, s);
+    if (m.wstart) launch_rows_mixed(m, x, y, s);
+    else launch_impl<float, float, float, double, double>(m, x, y, s);
 }
 
 }  // namespace spc5cuda

@@ -1,0 +1,429 @@
+// spmv_rows.cu -- thread-per-sub-row beta(r,VS) SpMV, y += A x, for
+// matrices whose block-rows are short (every block-row's headers and values
+// fit one per-warp staging buffer: stencils, Poisson, banded and FEM-like
+// matrices).
+//
+// Work split: warp w owns the contiguous block-rows [wstart[w], wstart[w+1])
+// (balanced by blocks).  It walks them in chunks of at most 32 / r
+// block-rows: the chunk's packed headers and values are copied into the
+// warp's shared-memory buffers with coalesced 16-byte cp.async, then lane
+// (k*r + s) computes sub-row s of the k-th block-row of the chunk on its
+// own.  All VS column accumulators of that sub-row live in the lane's
+// registers, so a block costs one header decode and VS predicated
+// multiply-adds per sub-row -- no shuffles, no per-block broadcasts.
+//
+// Arithmetic (bit-identical to the reference kernels core_SPC5_{r}rVc_Spmv_*,
+// src/spc5.hpp:2309-2715): accumulator c of sub-row s receives
+// fma(value, x[col + c], acc[c]) for every block in order whose mask s has
+// bit c, reading the values at the sub-row's compact offset in the block
+// (the masks of the sub-rows below s, then popcount of the bits below c) --
+// the expand-load of the vector kernel.  The row sum is the
+// _mm512_reduce_add tree over the accumulators (distance VS/2, then VS/4,
+// ..., 1) and y[row] += sum.  Clear bits skip the FMA, which leaves the
+// accumulator unchanged for finite x (it starts at +0.0 and never becomes
+// -0.0), so y is bit-identical for finite x.
+#include <algorithm>
+#include <climits>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace spc5cuda {
+
+namespace {
+
+constexpr int ROWS_THREADS = 128;
+constexpr int ROWS_WARPS = ROWS_THREADS / 32;
+constexpr int ROWS_CTAS_PER_SM = 16;
+constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ void cp_async16(uint32_t saddr, const void* gptr) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(gptr) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+// Waits until at most one committed group of this thread is still in flight.
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// Bulk prefetch of [p, p + bytes) into L2 (p 16-byte aligned, bytes a
+// multiple of 16); no data is returned.
+__device__ __forceinline__ void l2_prefetch(const void* p, uint32_t bytes) {
+    if (bytes) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
+}
+
+template <class LT, int R, class V>
+struct RowGeo {
+    static constexpr int VS = Layout<LT>::VS;
+    static constexpr int MB = Layout<LT>::MASK_BYTES;
+    static constexpr int STRIDE = Header<LT, R>::STRIDE;
+    static constexpr int MW = Header<LT, R>::MASK_WORDS;
+    static constexpr int LOAD_WORDS = Header<LT, R>::LOAD_WORDS;
+    static constexpr int SPW = 32 / R;   // block-rows per chunk (one per r lanes)
+    static constexpr int HB = 2048;      // header bytes per warp buffer
+    static constexpr int VB = 8192;      // value bytes per warp buffer
+    static constexpr int EPU = 16 / int(sizeof(V));
+    static constexpr int BUF_BYTES = HB + VB;
+    static constexpr int WARP_BYTES = BUF_BYTES;
+    static constexpr int SMEM = ROWS_WARPS * WARP_BYTES;
+};
+
+// One chunk of a warp's range: block-rows r0 .. r0 + nrow - 1 (at most
+// 32 / r), small enough for one staging buffer.  Lane k < nrow holds the end
+// block and end value of block-row r0 + k.
+struct Chunk {
+    int r0, nrow;
+    int b_lo, v_lo;  // first block and first value of the chunk
+    long h_al;       // 16-byte aligned start of the chunk's header bytes
+    int v_al;        // start of the chunk's values, rounded down to 16 bytes
+    int b_hi, v_hi;  // this lane's block-row end (lane < nrow)
+    int hunits, vunits;
+};
+
+template <class LT, int R, class V, class X, class A, class Y>
+__global__ void __launch_bounds__(ROWS_THREADS)
+    k_rows(int nrows, const int* __restrict__ brptr, const uint8_t* __restrict__ headers,
+           const V* __restrict__ values, const int* __restrict__ valptr,
+           const int* __restrict__ wstart, int nwarps, const X* __restrict__ x, Y* __restrict__ y) {
+    using G = RowGeo<LT, R, V>;
+    constexpr int VS = G::VS, MB = G::MB, S = G::STRIDE, MW = G::MW, SPW = G::SPW, EPU = G::EPU;
+    constexpr int FPW = 4 / MB;  // mask fields per 32-bit word
+    constexpr int BITS = 8 * MB;
+    constexpr uint32_t FMASK = MB == 1 ? 0xFFu : 0xFFFFu;
+    constexpr bool Y_ATOMIC = sizeof(Y) == 8;  // red.add.f64 is y + s rounded once
+    extern __shared__ __align__(16) unsigned char smem[];
+
+    const int lane = threadIdx.x & 31;
+    const int wi = threadIdx.x >> 5;
+    const int warp = blockIdx.x * ROWS_WARPS + wi;
+    const int slot = lane / R;
+    const int sub = lane % R;
+    unsigned char* wbuf = smem + wi * G::WARP_BYTES;  // two buffers: [headers | values] x 2
+    const uint32_t s_w = uint32_t(__cvta_generic_to_shared(wbuf));
+
+    int r_begin = 0, r_stop = 0;
+    if (warp < nwarps) {
+        r_begin = __ldg(wstart + warp);
+        r_stop = __ldg(wstart + warp + 1);
+    }
+    if (r_begin >= r_stop) return;  // warp-uniform
+    // end of this warp's header bytes and values: prefetches stay inside
+    const long h_stop = (long(__ldg(brptr + r_stop)) * S + 15) & ~15L;
+    const long v_stop = (long(__ldg(valptr + r_stop)) + EPU - 1) & ~long(EPU - 1);
+
+    // ---- the chunk starting at block-row r0 (nrow = 0 past the range).
+    // bounds() issues the loads of the block-row ends (lane k: block-row
+    // r0 + k), finish() decides how many block-rows fit the buffers; the
+    // loads of the next chunk are issued a chunk ahead of their use.
+    struct Bounds {
+        int r0, b_lo, v_lo, b_hi, v_hi;
+        bool cand;
+    };
+    auto bounds = [&](int r0, int b_lo, int v_lo) {
+        Bounds bd;
+        bd.r0 = r0;
+        bd.b_lo = b_lo;
+        bd.v_lo = v_lo;
+        bd.cand = lane < SPW && r0 + lane < r_stop;
+        bd.b_hi = bd.cand ? __ldg(brptr + r0 + lane + 1) : 0;
+        bd.v_hi = bd.cand ? __ldg(valptr + r0 + lane + 1) : 0;
+        return bd;
+    };
+    auto finish = [&](const Bounds& bd) {
+        Chunk ch;
+        ch.r0 = bd.r0;
+        ch.b_lo = bd.b_lo;
+        ch.v_lo = bd.v_lo;
+        ch.b_hi = bd.b_hi;
+        ch.v_hi = bd.v_hi;
+        ch.h_al = (long(ch.b_lo) * S) & ~15L;
+        ch.v_al = ch.v_lo & ~(EPU - 1);
+        bool fits = false;
+        if (bd.cand) {
+            const long hneed = ((long(ch.b_hi) * S + 15) & ~15L) - ch.h_al;
+            const long vneed = long((ch.v_hi + EPU - 1) & ~(EPU - 1)) - ch.v_al;
+            fits = hneed <= G::HB && vneed * long(sizeof(V)) <= G::VB;
+        }
+        // the ends grow with the lane, so the fitting lanes are a prefix; the
+        // host admits only matrices whose every block-row fits alone
+        ch.nrow = __popc(__ballot_sync(FULL, fits));
+        const int last = ch.nrow > 0 ? ch.nrow - 1 : 0;
+        const int b_end = __shfl_sync(FULL, ch.b_hi, last);
+        const int v_end = __shfl_sync(FULL, ch.v_hi, last);
+        ch.hunits = 0;
+        ch.vunits = 0;
+        if (ch.nrow > 0) {
+            ch.hunits = int((((long(b_end) * S + 15) & ~15L) - ch.h_al) >> 4);
+            ch.vunits = (v_end - ch.v_al + EPU - 1) / EPU;
+        }
+        return ch;
+    };
+
+    // ---- copy a chunk's headers and values into buffer bi (one commit group)
+    auto stage = [&](const Chunk& ch, int bi) {
+        const uint32_t s_h = s_w + uint32_t(bi * G::BUF_BYTES);
+        const uint32_t s_v = s_h + uint32_t(G::HB);
+        const uint8_t* hsrc = headers + ch.h_al;
+        for (int u = lane; u < ch.hunits; u += 32) cp_async16(s_h + 16u * uint32_t(u), hsrc + 16L * u);
+        const V* vsrc = values + ch.v_al;
+        for (int u = lane; u < ch.vunits; u += 32) cp_async16(s_v + 16u * uint32_t(u), vsrc + long(u) * EPU);
+        cp_async_commit();
+        // warm L2 with the data after this chunk (the next one is about as
+        // large), clipped to this warp's range
+        if (lane == 0 && ch.nrow > 0 && ch.r0 + ch.nrow < r_stop) {
+            const long h0 = ch.h_al + 16L * ch.hunits;
+            const long hn = std::min(16L * ch.hunits, h_stop - h0);
+            if (hn > 0) l2_prefetch(headers + h0, uint32_t(hn));
+            const long v0 = long(ch.v_al) + long(ch.vunits) * EPU;
+            const long vn = std::min(long(ch.vunits) * EPU, v_stop - v0);
+            if (vn > 0) l2_prefetch(values + v0, uint32_t(vn * long(sizeof(V))));
+        }
+    };
+
+    // ---- sub-row `sub` of block-row r0 + slot of a staged chunk
+    auto compute = [&](const Chunk& ch, int bi) {
+        const uint32_t* hw = reinterpret_cast<const uint32_t*>(wbuf + bi * G::BUF_BYTES);
+        const V* vbuf = reinterpret_cast<const V*>(wbuf + bi * G::BUF_BYTES + G::HB);
+        const int src = slot > 0 ? slot - 1 : 0;
+        const int b_prev = __shfl_sync(FULL, ch.b_hi, src);
+        const int v_prev = __shfl_sync(FULL, ch.v_hi, src);
+        const int b_mine = __shfl_sync(FULL, ch.b_hi, slot);
+        const bool mine = slot < ch.nrow;
+        int b = mine ? (slot > 0 ? b_prev : ch.b_lo) : 0;
+        const int b_stop = mine ? b_mine : 0;
+        int v = (mine ? (slot > 0 ? v_prev : ch.v_lo) : 0) - ch.v_al;  // buffer index of the block's values
+
+        // Header of block bb from the staged records: column, this sub-row's
+        // mask, the values of the sub-rows below it and of the whole block.
+        auto decode = [&](int bb, int& col, uint32_t& m, int& pre, int& tot) {
+            const long off = long(bb) * S - ch.h_al;
+            uint32_t lw[G::LOAD_WORDS + 1];
+#pragma unroll
+            for (int q = 0; q < G::LOAD_WORDS; ++q) lw[q] = hw[(off >> 2) + q];
+            lw[G::LOAD_WORDS] = 0u;
+            uint32_t mw[MW];
+            if constexpr (S % 4 == 0) {
+                col = int(lw[0]);
+#pragma unroll
+                for (int q = 0; q < MW; ++q) mw[q] = lw[1 + q];
+            } else {
+                const unsigned sh = unsigned(off & 3) * 8u;
+                col = int(__funnelshift_r(lw[0], lw[1], sh));
+                mw[0] = __funnelshift_r(lw[1], lw[2], sh) &
+                        ((1u << (8 * Header<LT, R>::MASK_BYTES_TOTAL)) - 1u);
+            }
+            m = 0;
+            pre = 0;
+            tot = 0;
+#pragma unroll
+            for (int q = 0; q < MW; ++q) {
+                const int pc = __popc(mw[q]);
+                tot += pc;
+                if constexpr (R > 1) {
+                    const int f0 = q * FPW;
+                    if (sub >= f0 + FPW) {
+                        pre += pc;
+                    } else if (sub >= f0) {
+                        const int fs = sub - f0;
+                        m = (mw[q] >> (BITS * fs)) & FMASK;
+                        pre += __popc(mw[q] & ((1u << (BITS * fs)) - 1u));
+                    }
+                } else {
+                    m = mw[q] & FMASK;
+                }
+            }
+        };
+
+        A acc[VS];
+#pragma unroll
+        for (int c = 0; c < VS; ++c) acc[c] = A(0);
+
+        // U blocks per step (two for 8-column blocks): the x loads of all of
+        // them are issued before the FMAs, which still run block by block
+        // (the chain order is kept).
+        constexpr int U = VS == 8 ? 2 : 1;
+        while (__any_sync(FULL, b < b_stop)) {
+            int col[U], pre[U], tot[U];
+            uint32_t m[U];
+#pragma unroll
+            for (int k = 0; k < U; ++k) {
+                col[k] = 0;
+                pre[k] = 0;
+                tot[k] = 0;
+                m[k] = 0;
+                if (b + k < b_stop) decode(b + k, col[k], m[k], pre[k], tot[k]);
+            }
+            X xk[U][VS];
+#pragma unroll
+            for (int k = 0; k < U; ++k) {
+                const X* xp = x + col[k];
+#pragma unroll
+                for (int c = 0; c < VS; ++c) xk[k][c] = ((m[k] >> c) & 1u) ? __ldg(xp + c) : X(0);
+            }
+#pragma unroll
+            for (int k = 0; k < U; ++k) {
+                int vi = v + pre[k];
+#pragma unroll
+                for (int c = 0; c < VS; ++c) {
+                    if ((m[k] >> c) & 1u) {
+                        acc[c] = fma(A(vbuf[vi]), A(xk[k][c]), acc[c]);
+                        ++vi;
+                    }
+                }
+                v += tot[k];
+            }
+            b += U;
+        }
+        // ---- row sums: the _mm512_reduce_add tree, then y += sum
+        if (mine) {
+#pragma unroll
+            for (int d = VS / 2; d >= 1; d >>= 1) {
+#pragma unroll
+                for (int e = 0; e < d; ++e) acc[e] = acc[e] + acc[e + d];
+            }
+            const long yrow = long(ch.r0 + slot) * R + sub;
+            if (yrow < nrows) {
+                if constexpr (Y_ATOMIC) atomicAdd(y + yrow, Y(acc[0]));
+                else y[yrow] = y[yrow] + Y(acc[0]);
+            }
+        }
+    };
+
+    // ---- walk the range: copy a chunk, load the next chunk's bounds while
+    // the copies fly, compute, repeat
+    Chunk cur = finish(bounds(r_begin, __ldg(brptr + r_begin), __ldg(valptr + r_begin)));
+    while (cur.nrow > 0) {  // warp-uniform
+        stage(cur, 0);
+        const int last = cur.nrow - 1;
+        const int r_next = cur.r0 + cur.nrow;
+        const Bounds nb = bounds(r_next, __shfl_sync(FULL, cur.b_hi, last), __shfl_sync(FULL, cur.v_hi, last));
+        cp_async_wait_all();
+        __syncwarp();
+        compute(cur, 0);
+        __syncwarp();  // the next chunk overwrites the buffer
+        cur = r_next < r_stop ? finish(nb) : Chunk{r_next, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    }
+    cp_async_wait_all();
+}
+
+template <class K>
+void set_smem(K kernel, int bytes) {
+    SPC5_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+}
+
+template <class LT, class V, class X, class A, class Y>
+int rows_occupancy(int r) {
+    int n = 0;
+#define SPC5_ROCC(R_)                                                                              \
+    {                                                                                              \
+        using G = RowGeo<LT, R_, V>;                                                               \
+        auto kern = k_rows<LT, R_, V, X, A, Y>;                                                    \
+        set_smem(kern, G::SMEM);                                                                   \
+        SPC5_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, ROWS_THREADS, G::SMEM)); \
+    }
+    switch (r) {
+        case 1: SPC5_ROCC(1); break;
+        case 2: SPC5_ROCC(2); break;
+        case 4: SPC5_ROCC(4); break;
+        case 8: SPC5_ROCC(8); break;
+        default: throw Error(SPC5CUDA_ERR_FORMAT, "r must be 1, 2, 4 or 8");
+    }
+#undef SPC5_ROCC
+    return std::max(1, std::min(n, ROWS_CTAS_PER_SM));
+}
+
+template <class LT, class V, class X, class A, class Y>
+void launch_rows_impl(const BetaView& m, const X* x, Y* y, cudaStream_t s) {
+    if (m.nbr <= 0 || m.nwarps <= 0) return;
+    const V* vals = static_cast<const V*>(m.values);
+    const int ctas = (m.nwarps + ROWS_WARPS - 1) / ROWS_WARPS;
+#define SPC5_RLAUNCH(R_)                                                                       \
+    {                                                                                          \
+        using G = RowGeo<LT, R_, V>;                                                           \
+        auto kern = k_rows<LT, R_, V, X, A, Y>;                                                \
+        set_smem(kern, G::SMEM);                                                               \
+        kern<<<ctas, ROWS_THREADS, G::SMEM, s>>>(m.nrows, m.brptr, m.headers, vals, m.valptr,  \
+                                                 m.wstart, m.nwarps, x, y);                    \
+    }
+    switch (m.r) {
+        case 1: SPC5_RLAUNCH(1); break;
+        case 2: SPC5_RLAUNCH(2); break;
+        case 4: SPC5_RLAUNCH(4); break;
+        case 8: SPC5_RLAUNCH(8); break;
+        default: throw Error(SPC5CUDA_ERR_FORMAT, "r must be 1, 2, 4 or 8");
+    }
+#undef SPC5_RLAUNCH
+    SPC5_CUDA(cudaGetLastError());
+}
+
+// Largest block count and value count of any block-row.
+__global__ void k_blockrow_max(int nbr, const int* __restrict__ brptr, const int* __restrict__ valptr,
+                               int* __restrict__ out) {
+    int mb = 0, mv = 0;
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nbr; i += long(gridDim.x) * blockDim.x) {
+        mb = max(mb, brptr[i + 1] - brptr[i]);
+        mv = max(mv, valptr[i + 1] - valptr[i]);
+    }
+    for (int d = 16; d >= 1; d >>= 1) {
+        mb = max(mb, __shfl_xor_sync(FULL, mb, d));
+        mv = max(mv, __shfl_xor_sync(FULL, mv, d));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(out, mb);
+        atomicMax(out + 1, mv);
+    }
+}
+
+}  // namespace
+
+int rows_warps(int vs, int r) {
+    int per_sm;
+    if (vs == 8) {
+        per_sm = rows_occupancy<double, double, double, double, double>(r);
+    } else {
+        per_sm = std::min(rows_occupancy<float, float, float, float, float>(r),
+                          rows_occupancy<float, float, float, double, double>(r));
+    }
+    return sm_count() * per_sm * ROWS_WARPS;
+}
+
+bool rows_fit(int vs, int r, int max_blocks, int max_values) {
+    // every block-row alone must fit the staging buffers, alignment included
+    const int stride = 4 + r * (vs == 8 ? 1 : 2);
+    const int vbytes = vs == 8 ? 8 : 4;
+    const long hneed = long(max_blocks) * stride + 32;
+    const long vneed = (long(max_values) + 2 * (16 / vbytes)) * vbytes;
+    return hneed <= 2048 && vneed <= 8192;
+}
+
+void blockrow_max(int nbr, const int* brptr, const int* valptr, int* max_blocks, int* max_values,
+                  cudaStream_t s) {
+    int* d = nullptr;
+    SPC5_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d), 2 * sizeof(int), s));
+    SPC5_CUDA(cudaMemsetAsync(d, 0, 2 * sizeof(int), s));
+    if (nbr > 0) {
+        const int threads = 256;
+        const int blocks = std::max(1, std::min(div_up(nbr, threads), sm_count() * 4));
+        k_blockrow_max<<<blocks, threads, 0, s>>>(nbr, brptr, valptr, d);
+        SPC5_CUDA(cudaGetLastError());
+    }
+    int h[2] = {0, 0};
+    SPC5_CUDA(cudaMemcpyAsync(h, d, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    SPC5_CUDA(cudaFreeAsync(d, s));
+    SPC5_CUDA(cudaStreamSynchronize(s));
+    *max_blocks = h[0];
+    *max_values = h[1];
+}
+
+void launch_rows_f64(const BetaView& m, const double* x, double* y, cudaStream_t s) {
+    launch_rows_impl<double, double, double, double, double>(m, x, y, s);
+}
+
+void launch_rows_f32(const BetaView& m, const float* x, float* y, cudaStream_t s) {
+    launch_rows_impl<float, float, float, float, float>(m, x, y, s);
+}
+
+void launch_rows_mixed(const BetaView& m, const float* x, double* y, cudaStream_t s) {
+    launch_rows_impl<float, float, float, double, double>(m, x, y, s);
+}
+
+}  // namespace spc5cuda

@@ -136,6 +136,79 @@ def test_spmv_accumulates_like_oracle(cuda, tag, dt, r):
         assert y.cpu().numpy().tobytes() == yo.tobytes(), csr.name
 
 
+def kernel_cases():
+    yield from irregular_cases()
+    yield M.stencil27(24)
+    yield M.poisson2d(96)
+    yield M.random_csr(4000, 4000, 0.003, seed=11, empty_row_frac=0.5)  # runs of empty rows
+
+
+@pytest.mark.parametrize("tag,dt", DTYPES + [("mixed", np.float32)])
+@pytest.mark.parametrize("r", [1, 2, 4, 8])
+@pytest.mark.parametrize("kernel", [S.KERNEL_GROUPS, S.KERNEL_ROWS])
+def test_both_kernels_bit_exact(cuda, tag, dt, r, kernel):
+    """The group kernel and the thread-per-sub-row kernel each give the
+    oracle's bits (y += A x on a nonzero y); the row kernel refuses a matrix
+    with a block-row larger than its staging buffers."""
+    for csr in kernel_cases():
+        vals = csr.values.astype(dt)
+        brptr, headers, ov = oracle.csr_to_beta(r, csr.rowptr, csr.colidx, vals)
+        m = converted(csr, dt, r)
+        if kernel == S.KERNEL_ROWS:
+            nbr = len(brptr) - 1
+            longest = int(np.diff(brptr).max()) if nbr else 0
+            rp = csr.rowptr.astype(np.int64)
+            vals_per = rp[np.minimum(np.arange(1, nbr + 1) * r, csr.nrows)] - rp[np.arange(nbr) * r]
+            most = int(vals_per.max()) if nbr else 0
+            vb, mb = (8, 1) if dt == np.float64 else (4, 2)
+            fits = longest * (4 + r * mb) + 32 <= 2048 and (most + 2 * (16 // vb)) * vb <= 8192
+            try:
+                m.set_kernel(kernel)
+            except S.SPC5Error as e:
+                assert e.status == 5 and not fits, csr.name
+                continue
+            assert fits, csr.name
+        else:
+            m.set_kernel(kernel)
+        assert m.kernel == kernel, csr.name
+        x = M.x_vector(csr.ncols, 3, np.float32 if tag == "mixed" else dt)
+        if tag == "mixed":
+            y0 = M.x_vector(csr.nrows, 4)
+            yo = oracle.beta_spmv_mixed(r, csr.nrows, brptr, headers, ov, x, y0.copy())
+            y = dev(y0)
+            S.SPC5_Spmv_mixed(m, dev(x), y)
+        else:
+            y0 = M.x_vector(csr.nrows, 4, dt)
+            f = oracle.beta_spmv_f64 if dt == np.float64 else oracle.beta_spmv_f32
+            yo = f(r, csr.nrows, brptr, headers, ov, x, y0.copy())
+            y = dev(y0)
+            S.SPC5_Spmv(m, dev(x), y)
+        torch.cuda.synchronize()
+        assert y.cpu().numpy().tobytes() == yo.tobytes(), (csr.name, kernel)
+
+
+def test_kernel_selection(cuda):
+    """AUTO picks the row kernel for a stencil and the group kernel for a
+    matrix with a block-row longer than the row kernel's buffers."""
+    st = converted(M.stencil27(12), np.float64, 4)
+    assert st.kernel == S.KERNEL_ROWS
+    st.set_kernel(S.KERNEL_GROUPS)
+    assert st.kernel == S.KERNEL_GROUPS
+    st.set_kernel(S.KERNEL_AUTO)
+    assert st.kernel == S.KERNEL_ROWS
+    st8 = converted(M.stencil27(12), np.float64, 8)
+    assert st8.kernel == S.KERNEL_GROUPS  # AUTO keeps the group kernel at r = 8
+    st8.set_kernel(S.KERNEL_ROWS)
+    assert st8.kernel == S.KERNEL_ROWS
+    d = converted(M.dense(4096), np.float64, 1)  # one block-row of 512 blocks: 2.5 KB of headers
+    assert d.kernel == S.KERNEL_GROUPS
+    with pytest.raises(S.SPC5Error) as e:
+        d.set_kernel(S.KERNEL_ROWS)
+    assert e.value.status == 5
+    with pytest.raises(S.SPC5Error):
+        d.set_kernel(7)
+
+
 @pytest.mark.parametrize("r", [1, 2, 4, 8])
 def test_mixed_precision(cuda, r):
     for csr in list(irregular_cases())[:5]:
