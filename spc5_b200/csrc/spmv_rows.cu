@@ -95,9 +95,9 @@ __global__ void __launch_bounds__(ROWS_THREADS)
     const int lane = threadIdx.x & 31;
     const int wi = threadIdx.x >> 5;
     const int warp = blockIdx.x * ROWS_WARPS + wi;
-    const int slot = lane / R;
-    const int sub = lane % R;
-    unsigned char* wbuf = smem + wi * G::WARP_BYTES;  // two buffers: [headers | values] x 2
+    const int slot = lane / R;  // block-row of the chunk
+    const int q = lane % R;     // column class: this lane owns columns c = q + R k
+    unsigned char* wbuf = smem + wi * G::WARP_BYTES;
     const uint32_t s_w = uint32_t(__cvta_generic_to_shared(wbuf));
 
     int r_begin = 0, r_stop = 0;
@@ -181,6 +181,10 @@ __global__ void __launch_bounds__(ROWS_THREADS)
 
     // ---- sub-row `sub` of block-row r0 + slot of a staged chunk
     auto compute = [&](const Chunk& ch, int bi) {
+        constexpr int CPL = VS / R;  // columns per lane
+        // blocks per step: the x loads of all of them are issued before the
+        // FMAs, which still run block by block (the chain order is kept)
+        constexpr int U = R == 1 ? 2 : (R == 2 ? 4 : 8);
         const uint32_t* hw = reinterpret_cast<const uint32_t*>(wbuf + bi * G::BUF_BYTES);
         const V* vbuf = reinterpret_cast<const V*>(wbuf + bi * G::BUF_BYTES + G::HB);
         const int src = slot > 0 ? slot - 1 : 0;
@@ -192,98 +196,141 @@ __global__ void __launch_bounds__(ROWS_THREADS)
         const int b_stop = mine ? b_mine : 0;
         int v = (mine ? (slot > 0 ? v_prev : ch.v_lo) : 0) - ch.v_al;  // buffer index of the block's values
 
-        // Header of block bb from the staged records: column, this sub-row's
-        // mask, the values of the sub-rows below it and of the whole block.
-        auto decode = [&](int bb, int& col, uint32_t& m, int& pre, int& tot) {
+        // Header of block bb from the staged records: column and the mask
+        // words (mask of sub-row i in field i % FPW of word i / FPW).
+        auto decode = [&](int bb, int& col, uint32_t (&mw)[MW]) {
             const long off = long(bb) * S - ch.h_al;
             uint32_t lw[G::LOAD_WORDS + 1];
 #pragma unroll
-            for (int q = 0; q < G::LOAD_WORDS; ++q) lw[q] = hw[(off >> 2) + q];
+            for (int w = 0; w < G::LOAD_WORDS; ++w) lw[w] = hw[(off >> 2) + w];
             lw[G::LOAD_WORDS] = 0u;
-            uint32_t mw[MW];
             if constexpr (S % 4 == 0) {
                 col = int(lw[0]);
 #pragma unroll
-                for (int q = 0; q < MW; ++q) mw[q] = lw[1 + q];
+                for (int w = 0; w < MW; ++w) mw[w] = lw[1 + w];
             } else {
                 const unsigned sh = unsigned(off & 3) * 8u;
                 col = int(__funnelshift_r(lw[0], lw[1], sh));
                 mw[0] = __funnelshift_r(lw[1], lw[2], sh) &
                         ((1u << (8 * Header<LT, R>::MASK_BYTES_TOTAL)) - 1u);
             }
-            m = 0;
-            pre = 0;
-            tot = 0;
-#pragma unroll
-            for (int q = 0; q < MW; ++q) {
-                const int pc = __popc(mw[q]);
-                tot += pc;
-                if constexpr (R > 1) {
-                    const int f0 = q * FPW;
-                    if (sub >= f0 + FPW) {
-                        pre += pc;
-                    } else if (sub >= f0) {
-                        const int fs = sub - f0;
-                        m = (mw[q] >> (BITS * fs)) & FMASK;
-                        pre += __popc(mw[q] & ((1u << (BITS * fs)) - 1u));
-                    }
-                } else {
-                    m = mw[q] & FMASK;
-                }
-            }
         };
 
-        A acc[VS];
+        A acc[R][CPL];
 #pragma unroll
-        for (int c = 0; c < VS; ++c) acc[c] = A(0);
+        for (int i = 0; i < R; ++i)
+#pragma unroll
+            for (int k = 0; k < CPL; ++k) acc[i][k] = A(0);
 
-        // U blocks per step (two for 8-column blocks): the x loads of all of
-        // them are issued before the FMAs, which still run block by block
-        // (the chain order is kept).
-        constexpr int U = VS == 8 ? 2 : 1;
         while (__any_sync(FULL, b < b_stop)) {
-            int col[U], pre[U], tot[U];
-            uint32_t m[U];
+            int col[U];
+            uint32_t mw[U][MW];
 #pragma unroll
-            for (int k = 0; k < U; ++k) {
-                col[k] = 0;
-                pre[k] = 0;
-                tot[k] = 0;
-                m[k] = 0;
-                if (b + k < b_stop) decode(b + k, col[k], m[k], pre[k], tot[k]);
+            for (int u = 0; u < U; ++u) {
+                col[u] = 0;
+#pragma unroll
+                for (int w = 0; w < MW; ++w) mw[u][w] = 0u;
+                if (b + u < b_stop) decode(b + u, col[u], mw[u]);
             }
-            X xk[U][VS];
+            // x of this lane's columns where some sub-row has a value
+            X xk[U][CPL];
 #pragma unroll
-            for (int k = 0; k < U; ++k) {
-                const X* xp = x + col[k];
+            for (int u = 0; u < U; ++u) {
+                uint32_t uni = 0;
 #pragma unroll
-                for (int c = 0; c < VS; ++c) xk[k][c] = ((m[k] >> c) & 1u) ? __ldg(xp + c) : X(0);
+                for (int w = 0; w < MW; ++w) uni |= mw[u][w];
+                if constexpr (MB == 1) uni = (uni | (uni >> 16)) | ((uni | (uni >> 16)) >> 8);
+                else uni = uni | (uni >> 16);
+                const X* xp = x + col[u] + q;
+#pragma unroll
+                for (int k = 0; k < CPL; ++k)
+                    xk[u][k] = ((uni >> (q + R * k)) & 1u) ? __ldg(xp + R * k) : X(0);
             }
 #pragma unroll
-            for (int k = 0; k < U; ++k) {
-                int vi = v + pre[k];
+            for (int u = 0; u < U; ++u) {
+                // per mask word: exclusive prefix of the sub-row value counts,
+                // one field per sub-row
+                uint32_t pre[MW];
+                int tot = 0;
+                {
+                    uint32_t carry = 0;
 #pragma unroll
-                for (int c = 0; c < VS; ++c) {
-                    if ((m[k] >> c) & 1u) {
-                        acc[c] = fma(A(vbuf[vi]), A(xk[k][c]), acc[c]);
-                        ++vi;
+                    for (int w = 0; w < MW; ++w) {
+                        uint32_t cnt;
+                        if constexpr (MB == 1) {
+                            cnt = mw[u][w] - ((mw[u][w] >> 1) & 0x55555555u);
+                            cnt = (cnt & 0x33333333u) + ((cnt >> 2) & 0x33333333u);
+                            cnt = (cnt + (cnt >> 4)) & 0x0F0F0F0Fu;
+                            pre[w] = cnt * 0x01010100u + carry * 0x01010101u;
+                            carry += (cnt * 0x01010101u) >> 24;
+                        } else {
+                            cnt = mw[u][w] - ((mw[u][w] >> 1) & 0x55555555u);
+                            cnt = (cnt & 0x33333333u) + ((cnt >> 2) & 0x33333333u);
+                            cnt = (cnt + (cnt >> 4)) & 0x0F0F0F0Fu;
+                            cnt = (cnt + (cnt >> 8)) & 0x001F001Fu;
+                            pre[w] = (cnt << 16) + carry * 0x00010001u;
+                            carry += (cnt + (cnt >> 16)) & 0xFFFFu;
+                        }
+                    }
+                    tot = int(carry);
+                }
+#pragma unroll
+                for (int k = 0; k < CPL; ++k) {
+                    const int c = q + R * k;
+                    const uint32_t below = (1u << c) - 1u;
+#pragma unroll
+                    for (int w = 0; w < MW; ++w) {
+                        // field i: buffer offset of sub-row i's value in column c
+                        uint32_t off;
+                        if constexpr (R == 1) {
+                            off = uint32_t(__popc(mw[u][0] & below));
+                        } else if constexpr (MB == 1) {
+                            uint32_t t = mw[u][w] & (below * 0x01010101u);
+                            t = t - ((t >> 1) & 0x55555555u);
+                            t = (t & 0x33333333u) + ((t >> 2) & 0x33333333u);
+                            off = pre[w] + ((t + (t >> 4)) & 0x0F0F0F0Fu);
+                        } else {
+                            uint32_t t = mw[u][w] & (below * 0x00010001u);
+                            t = t - ((t >> 1) & 0x55555555u);
+                            t = (t & 0x33333333u) + ((t >> 2) & 0x33333333u);
+                            t = (t + (t >> 4)) & 0x0F0F0F0Fu;
+                            off = pre[w] + ((t + (t >> 8)) & 0x001F001Fu);
+                        }
+#pragma unroll
+                        for (int f = 0; f < FPW; ++f) {
+                            const int i = w * FPW + f;
+                            if (i < R && ((mw[u][w] >> (f * BITS + c)) & 1u)) {
+                                const int idx = v + int((off >> (f * BITS)) & FMASK);
+                                acc[i][k] = fma(A(vbuf[idx]), A(xk[u][k]), acc[i][k]);
+                            }
+                        }
                     }
                 }
-                v += tot[k];
+                v += tot;
             }
             b += U;
         }
-        // ---- row sums: the _mm512_reduce_add tree, then y += sum
-        if (mine) {
+        // ---- row sums: the _mm512_reduce_add tree (distance VS/2, ..., 1).
+        // Levels of distance >= R pair columns of the same class inside the
+        // lane; the last log2(R) levels pair the lanes of the block-row.
+        A res = A(0);
 #pragma unroll
-            for (int d = VS / 2; d >= 1; d >>= 1) {
+        for (int i = 0; i < R; ++i) {
 #pragma unroll
-                for (int e = 0; e < d; ++e) acc[e] = acc[e] + acc[e + d];
+            for (int d = CPL / 2; d >= 1; d >>= 1) {
+#pragma unroll
+                for (int k = 0; k < d; ++k) acc[i][k] = acc[i][k] + acc[i][k + d];
             }
-            const long yrow = long(ch.r0 + slot) * R + sub;
+            A sum = acc[i][0];
+#pragma unroll
+            for (int d = R / 2; d >= 1; d >>= 1) sum = sum + __shfl_xor_sync(FULL, sum, d);
+            if (i == q) res = sum;
+        }
+        if (mine) {
+            const long yrow = long(ch.r0 + slot) * R + q;
             if (yrow < nrows) {
-                if constexpr (Y_ATOMIC) atomicAdd(y + yrow, Y(acc[0]));
-                else y[yrow] = y[yrow] + Y(acc[0]);
+                if constexpr (Y_ATOMIC) atomicAdd(y + yrow, Y(res));
+                else y[yrow] = y[yrow] + Y(res);
             }
         }
     };
