@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(ROWS_THREADS)
         constexpr int CPL = VS / R;  // columns per lane
         // blocks per step: the x loads of all of them are issued before the
         // FMAs, which still run block by block (the chain order is kept)
-        constexpr int U = R == 1 ? 2 : (R == 2 ? 4 : 8);
+        constexpr int U = (R == 1 ? 2 : (R == 2 ? 4 : 8)) / (VS / 8);
         const uint32_t* hw = reinterpret_cast<const uint32_t*>(wbuf + bi * G::BUF_BYTES);
         const V* vbuf = reinterpret_cast<const V*>(wbuf + bi * G::BUF_BYTES + G::HB);
         const int src = slot > 0 ? slot - 1 : 0;
