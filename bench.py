@@ -96,10 +96,44 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.out = None
+        self.thread = None
+        self.rows = []
+        self.stop = False
+
+    # NVML clocks-event reason bits (nvml.h): read-only queries, nothing is set
+    _REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+                    "hw_thermal_slowdown": 0x40}
+
+    def _poll_nvml(self, h, nv):
+        try:
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        except Exception:
+            mx = None
+        while not self.stop:
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                try:
+                    bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                except Exception:
+                    bits = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+                self.rows.append((sm, mx, bits))
+            except Exception:
+                pass
+            time.sleep(0.002)
 
     def __enter__(self):
         try:
-            self.out = open(os.devnull if False else f"/tmp/spc5_clocks_{os.getpid()}.csv", "w")
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self.gpu)
+            import threading
+            self.thread = threading.Thread(target=self._poll_nvml, args=(h, nv), daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
+        try:
+            self.out = open(f"/tmp/spc5_clocks_{os.getpid()}.csv", "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-lms", "100"], stdout=self.out, stderr=subprocess.DEVNULL)
@@ -108,6 +142,9 @@ class ClockSampler:
         return self
 
     def __exit__(self, *a):
+        if self.thread is not None:
+            self.stop = True
+            self.thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -118,6 +155,15 @@ class ClockSampler:
             self.out.close()
 
     def summary(self):
+        if self.thread is not None:
+            if not self.rows:
+                return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "source": "nvml"}
+            sm = [r[0] for r in self.rows]
+            mx = [r[1] for r in self.rows if r[1]]
+            reasons = sorted({n for r in self.rows for n, b in self._REASON_BITS.items() if r[2] & b})
+            load = [v for v in sm if mx and v > 0.3 * max(mx)] or sm
+            return {"sm_mhz": statistics.median(load), "sm_max_mhz": max(mx) if mx else None,
+                    "reasons": reasons, "samples": len(self.rows), "source": "nvml, 2 ms"}
         path = f"/tmp/spc5_clocks_{os.getpid()}.csv"
         if not os.path.exists(path):
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
@@ -363,7 +409,7 @@ def run_gpu(args):
             if res is not None:
                 gbs, threads, nsteps, secs = res
                 cpu = {"value": round(gbs, 3), "unit": UNIT, "cores": threads, "kind": "reference",
-                       "sample": f"{nsteps} steps x {len(formats)} SPC5_Spmv_omp (r={formats}) on the full matrix, "
+                       "sample": f"{nsteps} steps x {len(FORMATS)} SPC5_Spmv_omp (r={list(FORMATS)}) on the full matrix, "
                                  f"{secs:.1f} s"}
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
