@@ -607,7 +607,7 @@ def run_serve(args):
 
 # spc5cuda_mat_kernel codes: SPC5CUDA_KERNEL_GROUPS = 1, SPC5CUDA_KERNEL_ROWS = 2
 KERNEL_NAME = {1: "k_spmv (group per block-row stream)", 2: "k_rows (thread per sub-row)",
-               0: "unconverted"}
+               3: "sorted plan (k_spmv + k_rows by block-row size)", 0: "unconverted"}
 
 
 def select_kernel(m, which):
@@ -615,6 +615,8 @@ def select_kernel(m, which):
     import spc5_b200 as S
     if which == "groups":
         m.set_kernel(S.KERNEL_GROUPS)
+    elif which == "sorted":
+        m.set_kernel(S.KERNEL_SORTED)
     elif which == "rows":
         try:
             m.set_kernel(S.KERNEL_ROWS)
@@ -639,7 +641,7 @@ def main():
     ap.add_argument("--formats", default="1,2,4,8", help="comma list of r to run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
-    ap.add_argument("--kernel", choices=["auto", "groups", "rows"], default="auto",
+    ap.add_argument("--kernel", choices=["auto", "groups", "rows", "sorted"], default="auto",
                     help="SpMV kernel (rows falls back to auto where a block-row does not fit)")
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu dram bytes per launch of the dominant kernel, if captured")

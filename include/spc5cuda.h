@@ -180,16 +180,24 @@ SPC5CUDA_API spc5cuda_status spc5cuda_mat_info(const spc5cuda_mat* mat, spc5cuda
  * kernel per r and instruction set).  Both kernels give the same bits.
  *   AUTO   -- for r <= 4, the thread-per-sub-row kernel when every
  *             block-row fits its per-warp staging buffers (stencils, Poisson,
- *             banded); otherwise the group kernel (one group of VS lanes per
- *             block-row stream);
+ *             banded); the length-sorted plan (below) when some block-row
+ *             does not; otherwise the group kernel (one group of VS lanes
+ *             per block-row stream);
  *   GROUPS -- always the group kernel;
  *   ROWS   -- the thread-per-sub-row kernel; SPC5CUDA_ERR_UNSUPPORTED on a
- *             converted matrix with a block-row that does not fit.
- * spc5cuda_mat_kernel reports the kernel SpMV uses now (GROUPS or ROWS; AUTO
- * before conversion). */
+ *             converted matrix with a block-row that does not fit;
+ *   SORTED -- the length-sorted plan: the handle keeps a second copy of the
+ *             matrix with its block-rows sorted by size, and SpMV runs each
+ *             size class with the kernel and lanes per block-row that suit
+ *             it.  AUTO uses it when some block-row does not fit the row
+ *             kernel (power-law and other irregular matrices).
+ * spc5cuda_mat_kernel reports the kernel SpMV uses now (GROUPS, ROWS or
+ * SORTED; AUTO before conversion).  Selecting SORTED on a converted matrix
+ * builds the sorted copy and synchronises the device. */
 #define SPC5CUDA_KERNEL_AUTO 0
 #define SPC5CUDA_KERNEL_GROUPS 1
 #define SPC5CUDA_KERNEL_ROWS 2
+#define SPC5CUDA_KERNEL_SORTED 3
 SPC5CUDA_API spc5cuda_status spc5cuda_mat_set_kernel(spc5cuda_mat* mat, int kernel);
 SPC5CUDA_API spc5cuda_status spc5cuda_mat_kernel(const spc5cuda_mat* mat, int* kernel);
 

@@ -59,6 +59,7 @@ TUNE_MEASURE = 1
 KERNEL_AUTO = 0
 KERNEL_GROUPS = 1
 KERNEL_ROWS = 2
+KERNEL_SORTED = 3
 
 
 class SPC5Error(RuntimeError):
@@ -243,12 +244,13 @@ class SPC5Mat:
         return inf
 
     def set_kernel(self, kernel: int) -> None:
-        """Select the SpMV kernel: KERNEL_AUTO, KERNEL_GROUPS or KERNEL_ROWS."""
+        """Select the SpMV kernel: KERNEL_AUTO, KERNEL_GROUPS, KERNEL_ROWS or KERNEL_SORTED."""
         _check(_lib().spc5cuda_mat_set_kernel(self._h, int(kernel)), "spc5cuda_mat_set_kernel")
 
     @property
     def kernel(self) -> int:
-        """The SpMV kernel in use: KERNEL_GROUPS or KERNEL_ROWS (KERNEL_AUTO before conversion)."""
+        """The SpMV kernel in use: KERNEL_GROUPS, KERNEL_ROWS or KERNEL_SORTED (KERNEL_AUTO before
+        conversion)."""
         k = C.c_int(0)
         _check(_lib().spc5cuda_mat_kernel(self._h, C.byref(k)), "spc5cuda_mat_kernel")
         return k.value

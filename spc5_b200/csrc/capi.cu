@@ -271,11 +271,14 @@ spc5cuda_status spc5cuda_mat_set_kernel(spc5cuda_mat* m, int kernel) {
     return guarded([&] {
         require(m, SPC5CUDA_ERR_INVALID, "null");
         require(kernel == SPC5CUDA_KERNEL_AUTO || kernel == SPC5CUDA_KERNEL_GROUPS ||
-                    kernel == SPC5CUDA_KERNEL_ROWS,
+                    kernel == SPC5CUDA_KERNEL_ROWS || kernel == SPC5CUDA_KERNEL_SORTED,
                 SPC5CUDA_ERR_INVALID, "unknown kernel");
         if (kernel == SPC5CUDA_KERNEL_ROWS && m->r != 0)
             require(m->rows_ok, SPC5CUDA_ERR_UNSUPPORTED, "a block-row exceeds the row kernel's buffers");
         m->kernel = kernel;
+        if (m->r != 0 && m->wants_plan() && !m->plan) {
+            build_sorted_plan(m, nullptr);
+        }
     });
 }
 
@@ -283,6 +286,7 @@ spc5cuda_status spc5cuda_mat_kernel(const spc5cuda_mat* m, int* kernel) {
     return guarded([&] {
         require(m && kernel, SPC5CUDA_ERR_INVALID, "null");
         if (m->r == 0) *kernel = SPC5CUDA_KERNEL_AUTO;
+        else if (m->use_plan()) *kernel = SPC5CUDA_KERNEL_SORTED;
         else *kernel = m->use_rows() ? SPC5CUDA_KERNEL_ROWS : SPC5CUDA_KERNEL_GROUPS;
     });
 }
@@ -362,10 +366,13 @@ spc5cuda_status spc5cuda_spmv(const spc5cuda_mat* m, const void* x, void* y, voi
         if (m->nrows == 0) return;
         require(x && y, SPC5CUDA_ERR_INVALID, "null vector");
         cudaStream_t s = static_cast<cudaStream_t>(stream);
-        if (m->value_type == SPC5CUDA_F64)
+        if (m->use_plan()) {
+            plan_spmv(m, x, y, false, s);
+        } else if (m->value_type == SPC5CUDA_F64) {
             launch_spmv_f64(m->view(), static_cast<const double*>(x), static_cast<double*>(y), s);
-        else
+        } else {
             launch_spmv_f32(m->view(), static_cast<const float*>(x), static_cast<float*>(y), s);
+        }
     });
 }
 
@@ -378,7 +385,12 @@ spc5cuda_status spc5cuda_spmv_mixed(const spc5cuda_mat* m, const float* x, doubl
                 "mixed precision needs an F32 matrix");
         if (m->nrows == 0) return;
         require(x && y, SPC5CUDA_ERR_INVALID, "null vector");
-        launch_spmv_mixed(m->view(), x, y, static_cast<cudaStream_t>(stream));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        if (m->use_plan()) {
+            plan_spmv(m, x, y, true, s);
+        } else {
+            launch_spmv_mixed(m->view(), x, y, s);
+        }
     });
 }
 

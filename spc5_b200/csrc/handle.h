@@ -4,7 +4,9 @@
 
 #include <cuda_runtime.h>
 
+#include <memory>
 #include <new>
+#include <vector>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -110,6 +112,36 @@ inline void require(bool cond, spc5cuda_status s, const char* what) {
 }
 
 
+// One part of the length-sorted plan: sorted block-rows [a, b), run by the
+// row kernel with `lanes` lanes per block-row (split: one range per warp), or
+// by the group kernel when lanes == 0 (split: one range per group); split
+// holds nsplit + 1 block-row starts.
+struct SpmvPart {
+    int lanes = 0;
+    int a = 0, b = 0;
+    Owned split;
+    int nsplit = 0;
+};
+
+// A copy of the matrix with its block-rows sorted by size (plan.cu).
+struct SortedPlan {
+    Owned sbrptr, sheaders, svalues, svalptr, perm;
+    std::vector<SpmvPart> parts;
+    long bytes() const {
+        long n = long(sbrptr.bytes + sheaders.bytes + svalues.bytes + svalptr.bytes + perm.bytes);
+        for (const auto& p : parts) n += long(p.split.bytes);
+        return n;
+    }
+};
+
+// The length-sorted plan of a converted matrix (plan.cu; synchronises s),
+// and the view of one of its parts.
+void build_sorted_plan(spc5cuda_mat* m, cudaStream_t s);
+BetaView plan_view(const spc5cuda_mat* m, const SpmvPart& part);
+// y += A x through the plan (x, y of the handle's types; mixed: F32 handle,
+// float x, double y).
+void plan_spmv(const spc5cuda_mat* m, const void* x, void* y, bool mixed, cudaStream_t s);
+
 }  // namespace spc5cuda
 
 // The device-resident SPC5Mat<T> (src/spc5.hpp:44-62).
@@ -134,6 +166,7 @@ struct spc5cuda_mat {
     int nwarps = 0;
     int kernel = SPC5CUDA_KERNEL_AUTO;  // SpMV kernel choice (spc5cuda_mat_set_kernel)
     bool rows_ok = false;               // every block-row fits the row kernel's buffers
+    std::unique_ptr<spc5cuda::SortedPlan> plan;  // length-sorted copy (irregular matrices)
 
     int nbr() const { return r ? spc5cuda::div_up(nrows, r) : 0; }
     BetaView view() const {
@@ -162,9 +195,18 @@ struct spc5cuda_mat {
         if (kernel == SPC5CUDA_KERNEL_ROWS) return true;
         return kernel == SPC5CUDA_KERNEL_AUTO && r <= 4;
     }
+    // The length-sorted plan runs on request, or by default when some
+    // block-row is too large for the row kernel (irregular matrices).
+    bool use_plan() const {
+        if (!plan) return false;
+        return kernel == SPC5CUDA_KERNEL_SORTED || (kernel == SPC5CUDA_KERNEL_AUTO && !rows_ok);
+    }
+    bool wants_plan() const {
+        return kernel == SPC5CUDA_KERNEL_SORTED || (kernel == SPC5CUDA_KERNEL_AUTO && !rows_ok);
+    }
     long device_bytes() const {
         return long(rowptr.bytes + colidx.bytes + values.bytes + brptr.bytes + headers.bytes +
-                    valptr.bytes + gstart.bytes + wstart.bytes);
+                    valptr.bytes + gstart.bytes + wstart.bytes) + (plan ? plan->bytes() : 0L);
     }
     // The per-group block-row ranges for the current device.
     // The per-group block-row ranges for the current device, and the per-warp
@@ -185,6 +227,8 @@ struct spc5cuda_mat {
             nwarps = 0;
             wstart.release();
         }
+        plan.reset();
+        if (wants_plan()) spc5cuda::build_sorted_plan(this, s);
     }
 };
 

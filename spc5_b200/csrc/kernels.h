@@ -51,6 +51,10 @@ struct BetaView {
     // starts of the per-warp ranges; null selects the group kernel
     const int* wstart = nullptr;
     int nwarps = 0;
+    int lanes = 0;               // row kernel: lanes per block-row (0: r)
+    // block-row of y for each block-row of these arrays (null: the same);
+    // set when the arrays are a reordered copy of the matrix
+    const int* perm = nullptr;
 };
 
 // Number of VS-lane groups the SpMV kernels launch on the current device
@@ -59,6 +63,8 @@ int spmv_groups(int vs, int r);
 
 // gstart[0..ngroups] = block-row ranges holding ~nblocks/ngroups blocks each.
 void launch_partition(int nbr, const int* brptr, int ngroups, int* gstart, cudaStream_t s);
+// The same over block-rows [a, b): gstart[0] = a, gstart[ngroups] = b.
+void launch_partition_range(int a, int b, const int* brptr, int ngroups, int* gstart, cudaStream_t s);
 
 void launch_spmv_f64(const BetaView& m, const double* x, double* y, cudaStream_t s);
 
@@ -66,8 +72,13 @@ void launch_spmv_f64(const BetaView& m, const double* x, double* y, cudaStream_t
 // whether block-rows of at most max_blocks blocks / max_values values fit its
 // staging buffers, and the largest block-row of a converted matrix
 // (synchronises s).
-int rows_warps(int vs, int r);
+int rows_warps(int vs, int r, int lanes = 0);
 bool rows_fit(int vs, int r, int max_blocks, int max_values);
+// Size of a block-row in units of one lane's share of a row-kernel chunk:
+// the block-row fits a chunk of 32 / L block-rows with L lanes each when
+// rows_lane_units(...) <= L * rows_unit().
+long rows_lane_units(int vs, int r, int nblocks, int nvalues);
+long rows_unit();
 void blockrow_max(int nbr, const int* brptr, const int* valptr, int* max_blocks, int* max_values,
                   cudaStream_t s);
 void launch_rows_f64(const BetaView& m, const double* x, double* y, cudaStream_t s);

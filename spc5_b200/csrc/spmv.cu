@@ -192,8 +192,8 @@ template <class LT, int R, class V, class X, class A, class Y>
 __global__ void __launch_bounds__(128)
     k_spmv(int nrows, const int* __restrict__ brptr, const uint8_t* __restrict__ headers,
            const V* __restrict__ values, const int* __restrict__ valptr,
-           const int* __restrict__ gstart, int ngroups, const X* __restrict__ x,
-           Y* __restrict__ y) {
+           const int* __restrict__ gstart, int ngroups, const int* __restrict__ perm,
+           const X* __restrict__ x, Y* __restrict__ y) {
     using G = Geo<LT, R, V, A>;
     using F = Fields<G::MB>;
     constexpr int VS = G::VS, MW = G::MW, NW = G::NW, PW = F::PER_WORD;
@@ -269,7 +269,8 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
                 for (int e = 0; e < d; ++e) a[e] = a[e] + a[e + d];
             }
-            const long yrow = long(srow + c / R) * R + (c % R);
+            const int brow = perm ? __ldg(perm + srow + c / R) : srow + c / R;
+            const long yrow = long(brow) * R + (c % R);
             if (yrow < nrows) {
                 if constexpr (Y_ATOMIC) atomicAdd(y + yrow, Y(a[0]));
                 else y[yrow] = y[yrow] + Y(a[0]);
@@ -463,22 +464,23 @@ __global__ void __launch_bounds__(128)
     if (__any_sync(FULL, ns > 0)) reduce_batch(ns > 0);
 }
 
-// gstart[g] = first block-row whose first block lies in group g's share
-// [g * nblocks / G, (g+1) * nblocks / G); gstart[G] = nbr.
-__global__ void k_partition(int nbr, const int* __restrict__ brptr, int ngroups,
+// gstart[g] = first block-row of [a, b) whose first block lies in group g's
+// share [g * n / G, (g+1) * n / G) of the range's n blocks; gstart[G] = b.
+__global__ void k_partition(int a, int b, const int* __restrict__ brptr, int ngroups,
                             int* __restrict__ gstart) {
-    const long nblocks = brptr[nbr];
-    for (long rr = long(blockIdx.x) * blockDim.x + threadIdx.x; rr <= nbr;
+    const long base = brptr[a];
+    const long nblocks = long(brptr[b]) - base;
+    for (long rr = a + long(blockIdx.x) * blockDim.x + threadIdx.x; rr <= b;
          rr += long(gridDim.x) * blockDim.x) {
-        // bucket of block-row rr (nbr -> G); groups in (bucket(rr-1), bucket(rr)] start at rr
+        // bucket of block-row rr (b -> G); groups in (bucket(rr-1), bucket(rr)] start at rr
         auto bucket = [&](long q) -> long {
-            if (q >= nbr) return ngroups;
+            if (q >= b) return ngroups;
             if (nblocks == 0) return 0;
-            const long bk = (long(brptr[q]) * ngroups) / nblocks;
+            const long bk = ((long(brptr[q]) - base) * ngroups) / nblocks;
             return bk < ngroups ? bk : ngroups - 1;
         };
         const long hi = bucket(rr);
-        const long lo = rr == 0 ? -1 : bucket(rr - 1);
+        const long lo = rr == a ? -1 : bucket(rr - 1);
         for (long g = lo + 1; g <= hi && g <= ngroups; ++g) gstart[g] = int(rr);
     }
 }
@@ -499,7 +501,7 @@ void launch_impl(const BetaView& m, const X* x, Y* y, cudaStream_t s) {
         auto kern = k_spmv<LT, R_, V, X, A, Y>;                                                  \
         set_smem(kern, G::SMEM);                                                                 \
         kern<<<ctas, G::THREADS, G::SMEM, s>>>(m.nrows, m.brptr, m.headers, vals, m.valptr,      \
-                                               m.gstart, m.ngroups, x, y);                       \
+                                               m.gstart, m.ngroups, m.perm, x, y);               \
     }
     switch (m.r) {
         case 1: SPC5_LAUNCH(1); break;
@@ -566,7 +568,14 @@ int spmv_groups(int vs, int r) {
 void launch_partition(int nbr, const int* brptr, int ngroups, int* gstart, cudaStream_t s) {
     const int threads = 256;
     const int blocks = std::max(1, std::min(div_up(long(nbr) + 1, threads), sm_count() * 8));
-    k_partition<<<blocks, threads, 0, s>>>(nbr, brptr, ngroups, gstart);
+    k_partition<<<blocks, threads, 0, s>>>(0, nbr, brptr, ngroups, gstart);
+    SPC5_CUDA(cudaGetLastError());
+}
+
+void launch_partition_range(int a, int b, const int* brptr, int ngroups, int* gstart, cudaStream_t s) {
+    const int threads = 256;
+    const int blocks = std::max(1, std::min(div_up(long(b - a) + 1, threads), sm_count() * 8));
+    k_partition<<<blocks, threads, 0, s>>>(a, b, brptr, ngroups, gstart);
     SPC5_CUDA(cudaGetLastError());
 }
 

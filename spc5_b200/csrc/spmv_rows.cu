@@ -23,6 +23,7 @@
 // accumulator unchanged for finite x (it starts at +0.0 and never becomes
 // -0.0), so y is bit-identical for finite x.
 #include <algorithm>
+#include <type_traits>
 #include <climits>
 
 #include "common.cuh"
@@ -51,16 +52,17 @@ __device__ __forceinline__ void l2_prefetch(const void* p, uint32_t bytes) {
     if (bytes) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
 }
 
-template <class LT, int R, class V>
+template <class LT, int R, class V, int L>
 struct RowGeo {
     static constexpr int VS = Layout<LT>::VS;
     static constexpr int MB = Layout<LT>::MASK_BYTES;
     static constexpr int STRIDE = Header<LT, R>::STRIDE;
     static constexpr int MW = Header<LT, R>::MASK_WORDS;
     static constexpr int LOAD_WORDS = Header<LT, R>::LOAD_WORDS;
-    static constexpr int SPW = 32 / R;   // block-rows per chunk (one per r lanes)
-    static constexpr int HB = 2048;      // header bytes per warp buffer
-    static constexpr int VB = 8192;      // value bytes per warp buffer
+    static_assert(L >= R && L <= Layout<LT>::VS && 32 % L == 0, "lanes per block-row");
+    static constexpr int SPW = 32 / L;   // block-rows per chunk (L lanes each)
+    static constexpr int HB = 2048;      // header bytes per warp buffer (ROWS_HB)
+    static constexpr int VB = 8192;      // value bytes per warp buffer (ROWS_VB)
     static constexpr int EPU = 16 / int(sizeof(V));
     static constexpr int BUF_BYTES = HB + VB;
     static constexpr int WARP_BYTES = BUF_BYTES;
@@ -79,12 +81,13 @@ struct Chunk {
     int hunits, vunits;
 };
 
-template <class LT, int R, class V, class X, class A, class Y>
+template <class LT, int R, class V, class X, class A, class Y, int L>
 __global__ void __launch_bounds__(ROWS_THREADS)
     k_rows(int nrows, const int* __restrict__ brptr, const uint8_t* __restrict__ headers,
            const V* __restrict__ values, const int* __restrict__ valptr,
-           const int* __restrict__ wstart, int nwarps, const X* __restrict__ x, Y* __restrict__ y) {
-    using G = RowGeo<LT, R, V>;
+           const int* __restrict__ wstart, int nwarps, const int* __restrict__ perm,
+           const X* __restrict__ x, Y* __restrict__ y) {
+    using G = RowGeo<LT, R, V, L>;
     constexpr int VS = G::VS, MB = G::MB, S = G::STRIDE, MW = G::MW, SPW = G::SPW, EPU = G::EPU;
     constexpr int FPW = 4 / MB;  // mask fields per 32-bit word
     constexpr int BITS = 8 * MB;
@@ -95,8 +98,8 @@ __global__ void __launch_bounds__(ROWS_THREADS)
     const int lane = threadIdx.x & 31;
     const int wi = threadIdx.x >> 5;
     const int warp = blockIdx.x * ROWS_WARPS + wi;
-    const int slot = lane / R;  // block-row of the chunk
-    const int q = lane % R;     // column class: this lane owns columns c = q + R k
+    const int slot = lane / L;  // block-row of the chunk
+    const int q = lane % L;     // column class: this lane owns columns c = q + L k
     unsigned char* wbuf = smem + wi * G::WARP_BYTES;
     const uint32_t s_w = uint32_t(__cvta_generic_to_shared(wbuf));
 
@@ -181,10 +184,10 @@ __global__ void __launch_bounds__(ROWS_THREADS)
 
     // ---- sub-row `sub` of block-row r0 + slot of a staged chunk
     auto compute = [&](const Chunk& ch, int bi) {
-        constexpr int CPL = VS / R;  // columns per lane
+        constexpr int CPL = VS / L;  // columns per lane
         // blocks per step: the x loads of all of them are issued before the
         // FMAs, which still run block by block (the chain order is kept)
-        constexpr int U = (R == 1 ? 2 : (R == 2 ? 4 : 8)) / (VS / 8);
+        constexpr int U = (16 / CPL) < 1 ? 1 : ((16 / CPL) > 8 ? 8 : 16 / CPL);
         const uint32_t* hw = reinterpret_cast<const uint32_t*>(wbuf + bi * G::BUF_BYTES);
         const V* vbuf = reinterpret_cast<const V*>(wbuf + bi * G::BUF_BYTES + G::HB);
         const int src = slot > 0 ? slot - 1 : 0;
@@ -244,7 +247,7 @@ __global__ void __launch_bounds__(ROWS_THREADS)
                 const X* xp = x + col[u] + q;
 #pragma unroll
                 for (int k = 0; k < CPL; ++k)
-                    xk[u][k] = ((uni >> (q + R * k)) & 1u) ? __ldg(xp + R * k) : X(0);
+                    xk[u][k] = ((uni >> (q + L * k)) & 1u) ? __ldg(xp + L * k) : X(0);
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
@@ -276,7 +279,7 @@ __global__ void __launch_bounds__(ROWS_THREADS)
                 }
 #pragma unroll
                 for (int k = 0; k < CPL; ++k) {
-                    const int c = q + R * k;
+                    const int c = q + L * k;
                     const uint32_t below = (1u << c) - 1u;
 #pragma unroll
                     for (int w = 0; w < MW; ++w) {
@@ -311,8 +314,8 @@ __global__ void __launch_bounds__(ROWS_THREADS)
             b += U;
         }
         // ---- row sums: the _mm512_reduce_add tree (distance VS/2, ..., 1).
-        // Levels of distance >= R pair columns of the same class inside the
-        // lane; the last log2(R) levels pair the lanes of the block-row.
+        // Levels of distance >= L pair columns of the same class inside the
+        // lane; the last log2(L) levels pair the lanes of the block-row.
         A res = A(0);
 #pragma unroll
         for (int i = 0; i < R; ++i) {
@@ -323,11 +326,12 @@ __global__ void __launch_bounds__(ROWS_THREADS)
             }
             A sum = acc[i][0];
 #pragma unroll
-            for (int d = R / 2; d >= 1; d >>= 1) sum = sum + __shfl_xor_sync(FULL, sum, d);
+            for (int d = L / 2; d >= 1; d >>= 1) sum = sum + __shfl_xor_sync(FULL, sum, d);
             if (i == q) res = sum;
         }
-        if (mine) {
-            const long yrow = long(ch.r0 + slot) * R + q;
+        if (mine && q < R) {
+            const int brow = perm ? __ldg(perm + ch.r0 + slot) : ch.r0 + slot;
+            const long yrow = long(brow) * R + q;
             if (yrow < nrows) {
                 if constexpr (Y_ATOMIC) atomicAdd(y + yrow, Y(res));
                 else y[yrow] = y[yrow] + Y(res);
@@ -357,24 +361,54 @@ void set_smem(K kernel, int bytes) {
     SPC5_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
 }
 
-template <class LT, class V, class X, class A, class Y>
-int rows_occupancy(int r) {
-    int n = 0;
-#define SPC5_ROCC(R_)                                                                              \
-    {                                                                                              \
-        using G = RowGeo<LT, R_, V>;                                                               \
-        auto kern = k_rows<LT, R_, V, X, A, Y>;                                                    \
-        set_smem(kern, G::SMEM);                                                                   \
-        SPC5_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, ROWS_THREADS, G::SMEM)); \
-    }
+// Calls f(std::integral_constant<int, R>, std::integral_constant<int, L>)
+// for a supported (r, lanes-per-block-row) pair: L >= r, L in {1, 2, 4, 8}.
+template <class F>
+void dispatch_rl(int r, int lanes, F&& f) {
+    using std::integral_constant;
+    const int L = lanes ? lanes : r;
     switch (r) {
-        case 1: SPC5_ROCC(1); break;
-        case 2: SPC5_ROCC(2); break;
-        case 4: SPC5_ROCC(4); break;
-        case 8: SPC5_ROCC(8); break;
-        default: throw Error(SPC5CUDA_ERR_FORMAT, "r must be 1, 2, 4 or 8");
+        case 1:
+            switch (L) {
+                case 1: f(integral_constant<int, 1>{}, integral_constant<int, 1>{}); return;
+                case 2: f(integral_constant<int, 1>{}, integral_constant<int, 2>{}); return;
+                case 4: f(integral_constant<int, 1>{}, integral_constant<int, 4>{}); return;
+                case 8: f(integral_constant<int, 1>{}, integral_constant<int, 8>{}); return;
+            }
+            break;
+        case 2:
+            switch (L) {
+                case 2: f(integral_constant<int, 2>{}, integral_constant<int, 2>{}); return;
+                case 4: f(integral_constant<int, 2>{}, integral_constant<int, 4>{}); return;
+                case 8: f(integral_constant<int, 2>{}, integral_constant<int, 8>{}); return;
+            }
+            break;
+        case 4:
+            switch (L) {
+                case 4: f(integral_constant<int, 4>{}, integral_constant<int, 4>{}); return;
+                case 8: f(integral_constant<int, 4>{}, integral_constant<int, 8>{}); return;
+            }
+            break;
+        case 8:
+            if (L == 8) {
+                f(integral_constant<int, 8>{}, integral_constant<int, 8>{});
+                return;
+            }
+            break;
     }
-#undef SPC5_ROCC
+    throw Error(SPC5CUDA_ERR_FORMAT, "r must be 1, 2, 4 or 8 and lanes >= r");
+}
+
+template <class LT, class V, class X, class A, class Y>
+int rows_occupancy(int r, int lanes) {
+    int n = 0;
+    dispatch_rl(r, lanes, [&](auto RC, auto LC) {
+        constexpr int R_ = decltype(RC)::value, L_ = decltype(LC)::value;
+        using G = RowGeo<LT, R_, V, L_>;
+        auto kern = k_rows<LT, R_, V, X, A, Y, L_>;
+        set_smem(kern, G::SMEM);
+        SPC5_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, ROWS_THREADS, G::SMEM));
+    });
     return std::max(1, std::min(n, ROWS_CTAS_PER_SM));
 }
 
@@ -383,22 +417,14 @@ void launch_rows_impl(const BetaView& m, const X* x, Y* y, cudaStream_t s) {
     if (m.nbr <= 0 || m.nwarps <= 0) return;
     const V* vals = static_cast<const V*>(m.values);
     const int ctas = (m.nwarps + ROWS_WARPS - 1) / ROWS_WARPS;
-#define SPC5_RLAUNCH(R_)                                                                       \
-    {                                                                                          \
-        using G = RowGeo<LT, R_, V>;                                                           \
-        auto kern = k_rows<LT, R_, V, X, A, Y>;                                                \
-        set_smem(kern, G::SMEM);                                                               \
-        kern<<<ctas, ROWS_THREADS, G::SMEM, s>>>(m.nrows, m.brptr, m.headers, vals, m.valptr,  \
-                                                 m.wstart, m.nwarps, x, y);                    \
-    }
-    switch (m.r) {
-        case 1: SPC5_RLAUNCH(1); break;
-        case 2: SPC5_RLAUNCH(2); break;
-        case 4: SPC5_RLAUNCH(4); break;
-        case 8: SPC5_RLAUNCH(8); break;
-        default: throw Error(SPC5CUDA_ERR_FORMAT, "r must be 1, 2, 4 or 8");
-    }
-#undef SPC5_RLAUNCH
+    dispatch_rl(m.r, m.lanes, [&](auto RC, auto LC) {
+        constexpr int R_ = decltype(RC)::value, L_ = decltype(LC)::value;
+        using G = RowGeo<LT, R_, V, L_>;
+        auto kern = k_rows<LT, R_, V, X, A, Y, L_>;
+        set_smem(kern, G::SMEM);
+        kern<<<ctas, ROWS_THREADS, G::SMEM, s>>>(m.nrows, m.brptr, m.headers, vals, m.valptr, m.wstart,
+                                                 m.nwarps, m.perm, x, y);
+    });
     SPC5_CUDA(cudaGetLastError());
 }
 
@@ -422,16 +448,20 @@ __global__ void k_blockrow_max(int nbr, const int* __restrict__ brptr, const int
 
 }  // namespace
 
-int rows_warps(int vs, int r) {
+int rows_warps(int vs, int r, int lanes) {
     int per_sm;
     if (vs == 8) {
-        per_sm = rows_occupancy<double, double, double, double, double>(r);
+        per_sm = rows_occupancy<double, double, double, double, double>(r, lanes);
     } else {
-        per_sm = std::min(rows_occupancy<float, float, float, float, float>(r),
-                          rows_occupancy<float, float, float, double, double>(r));
+        per_sm = std::min(rows_occupancy<float, float, float, float, float>(r, lanes),
+                          rows_occupancy<float, float, float, double, double>(r, lanes));
     }
     return sm_count() * per_sm * ROWS_WARPS;
 }
+
+// Staging buffer sizes of RowGeo (every instantiation).
+constexpr int ROWS_HB = 2048;
+constexpr int ROWS_VB = 8192;
 
 bool rows_fit(int vs, int r, int max_blocks, int max_values) {
     // every block-row alone must fit the staging buffers, alignment included
@@ -439,8 +469,18 @@ bool rows_fit(int vs, int r, int max_blocks, int max_values) {
     const int vbytes = vs == 8 ? 8 : 4;
     const long hneed = long(max_blocks) * stride + 32;
     const long vneed = (long(max_values) + 2 * (16 / vbytes)) * vbytes;
-    return hneed <= 2048 && vneed <= 8192;
+    return hneed <= ROWS_HB && vneed <= ROWS_VB;
 }
+
+long rows_lane_units(int vs, int r, int nblocks, int nvalues) {
+    // a block-row of this size fits `lanes` lanes' share of a chunk (32 / lanes
+    // block-rows per chunk) when the result is <= lanes * ROWS_UNIT
+    const long stride = 4 + r * (vs == 8 ? 1 : 2);
+    const long vbytes = vs == 8 ? 8 : 4;
+    return std::max(long(nblocks) * stride * (ROWS_VB - 32), long(nvalues) * vbytes * (ROWS_HB - 32));
+}
+
+long rows_unit() { return long(ROWS_HB - 32) * long(ROWS_VB - 32) / 32; }
 
 void blockrow_max(int nbr, const int* brptr, const int* valptr, int* max_blocks, int* max_values,
                   cudaStream_t s) {

@@ -145,11 +145,12 @@ def kernel_cases():
 
 @pytest.mark.parametrize("tag,dt", DTYPES + [("mixed", np.float32)])
 @pytest.mark.parametrize("r", [1, 2, 4, 8])
-@pytest.mark.parametrize("kernel", [S.KERNEL_GROUPS, S.KERNEL_ROWS])
+@pytest.mark.parametrize("kernel", [S.KERNEL_GROUPS, S.KERNEL_ROWS, S.KERNEL_SORTED])
 def test_both_kernels_bit_exact(cuda, tag, dt, r, kernel):
-    """The group kernel and the thread-per-sub-row kernel each give the
-    oracle's bits (y += A x on a nonzero y); the row kernel refuses a matrix
-    with a block-row larger than its staging buffers."""
+    """The group kernel, the thread-per-sub-row kernel and the length-sorted
+    plan each give the oracle's bits (y += A x on a nonzero y); the row
+    kernel refuses a matrix with a block-row larger than its staging
+    buffers."""
     for csr in kernel_cases():
         vals = csr.values.astype(dt)
         brptr, headers, ov = oracle.csr_to_beta(r, csr.rowptr, csr.colidx, vals)
@@ -201,12 +202,19 @@ def test_kernel_selection(cuda):
     st8.set_kernel(S.KERNEL_ROWS)
     assert st8.kernel == S.KERNEL_ROWS
     d = converted(M.dense(4096), np.float64, 1)  # one block-row of 512 blocks: 2.5 KB of headers
+    assert d.kernel == S.KERNEL_SORTED  # AUTO: a block-row does not fit the row kernel
+    d.set_kernel(S.KERNEL_GROUPS)
     assert d.kernel == S.KERNEL_GROUPS
     with pytest.raises(S.SPC5Error) as e:
         d.set_kernel(S.KERNEL_ROWS)
     assert e.value.status == 5
     with pytest.raises(S.SPC5Error):
         d.set_kernel(7)
+    pl = converted(M.powerlaw(20000, seed=7), np.float64, 2)
+    assert pl.kernel == S.KERNEL_SORTED
+    before = pl.info().device_bytes
+    pl.set_kernel(S.KERNEL_GROUPS)
+    assert pl.kernel == S.KERNEL_GROUPS and pl.info().device_bytes == before  # the copy stays
 
 
 @pytest.mark.parametrize("r", [1, 2, 4, 8])
