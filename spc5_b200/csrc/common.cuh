@@ -98,4 +98,36 @@ __device__ __forceinline__ uint32_t mask_of(const uint32_t (&mw)[Header<T, R>::M
     return (word >> ((byte & 3) * 8)) & (MB == 1 ? 0xFFu : 0xFFFFu);
 }
 
+// L2 cache policies: the matrix is streamed once per SpMV and should not
+// push x out of L2; x is gathered many times and should stay.
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t l2_evict_last_policy() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+// 16-byte global -> shared asynchronous copy (L2 only) with an L2 policy.
+__device__ __forceinline__ void cp_async16_hint(uint32_t saddr, const void* gptr, uint64_t pol) {
+    asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;\n" ::"r"(saddr), "l"(gptr),
+                 "l"(pol)
+                 : "memory");
+}
+
+// Read-only load of an x element with an L2 policy.
+__device__ __forceinline__ double ld_x(const double* p, uint64_t pol) {
+    double v;
+    asm volatile("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float ld_x(const float* p, uint64_t pol) {
+    float v;
+    asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
 }  // namespace spc5cuda

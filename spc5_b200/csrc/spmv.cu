@@ -220,6 +220,8 @@ __global__ void __launch_bounds__(128)
         r_end = __ldg(gstart + group + 1);
     }
     if (!__any_sync(FULL, r_begin < r_end)) return;
+    const uint64_t pol_stream = l2_evict_first_policy();  // values: read once
+    const uint64_t pol_x = l2_evict_last_policy();        // x: gathered many times
     const bool has = r_begin < r_end;
     const int b_stop = has ? __ldg(brptr + r_end) : 0;
     int p = has ? __ldg(brptr + r_begin) : 0;  // first block of the next window to stage
@@ -349,7 +351,7 @@ __global__ void __launch_bounds__(128)
             const uint32_t vb = sgbase + uint32_t(bi * G::VBUF);
             const int units = (shift + tv + G::EPU - 1) / G::EPU;
             const V* src = values + s0;
-            for (int u = c; u < units; u += VS) cp_async16(vb + uint32_t(u) * 16u, src + u * G::EPU);
+            for (int u = c; u < units; u += VS) cp_async16_hint(vb + uint32_t(u) * 16u, src + u * G::EPU, pol_stream);
         }
         cp_async_commit();
         v_next += (n > 0) ? tv : 0;
@@ -390,7 +392,7 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
             for (int q = 0; q < MW; ++q) lanes |= F::fold(mask_word(wj, q));
             xv[j] = X(0);
-            if (j < cur.n && ((lanes >> c) & 1u)) xv[j] = __ldg(x + (cj + c));
+            if (j < cur.n && ((lanes >> c) & 1u)) xv[j] = ld_x(x + (cj + c), pol_x);
             if constexpr (KEEP) {
 #pragma unroll
                 for (int q = 0; q < NW; ++q) keep[j][q] = wj[q];

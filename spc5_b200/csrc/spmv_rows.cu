@@ -109,6 +109,8 @@ __global__ void __launch_bounds__(ROWS_THREADS)
         r_stop = __ldg(wstart + warp + 1);
     }
     if (r_begin >= r_stop) return;  // warp-uniform
+    const uint64_t pol_stream = l2_evict_first_policy();
+    const uint64_t pol_x = l2_evict_last_policy();
     // end of this warp's header bytes and values: prefetches stay inside
     const long h_stop = (long(__ldg(brptr + r_stop)) * S + 15) & ~15L;
     const long v_stop = (long(__ldg(valptr + r_stop)) + EPU - 1) & ~long(EPU - 1);
@@ -166,9 +168,9 @@ __global__ void __launch_bounds__(ROWS_THREADS)
         const uint32_t s_h = s_w + uint32_t(bi * G::BUF_BYTES);
         const uint32_t s_v = s_h + uint32_t(G::HB);
         const uint8_t* hsrc = headers + ch.h_al;
-        for (int u = lane; u < ch.hunits; u += 32) cp_async16(s_h + 16u * uint32_t(u), hsrc + 16L * u);
+        for (int u = lane; u < ch.hunits; u += 32) cp_async16_hint(s_h + 16u * uint32_t(u), hsrc + 16L * u, pol_stream);
         const V* vsrc = values + ch.v_al;
-        for (int u = lane; u < ch.vunits; u += 32) cp_async16(s_v + 16u * uint32_t(u), vsrc + long(u) * EPU);
+        for (int u = lane; u < ch.vunits; u += 32) cp_async16_hint(s_v + 16u * uint32_t(u), vsrc + long(u) * EPU, pol_stream);
         cp_async_commit();
         // warm L2 with the data after this chunk (the next one is about as
         // large), clipped to this warp's range
@@ -247,7 +249,7 @@ __global__ void __launch_bounds__(ROWS_THREADS)
                 const X* xp = x + col[u] + q;
 #pragma unroll
                 for (int k = 0; k < CPL; ++k)
-                    xk[u][k] = ((uni >> (q + L * k)) & 1u) ? __ldg(xp + L * k) : X(0);
+                    xk[u][k] = ((uni >> (q + L * k)) & 1u) ? ld_x(xp + L * k, pol_x) : X(0);
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
