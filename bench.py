@@ -109,6 +109,7 @@ class ClockSampler:
             mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
         except Exception:
             mx = None
+        self._mx = mx
         while not self.stop:
             try:
                 sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
@@ -129,6 +130,7 @@ class ClockSampler:
             import threading
             self.thread = threading.Thread(target=self._poll_nvml, args=(h, nv), daemon=True)
             self.thread.start()
+            self._h, self._nv = h, nv
             return self
         except Exception:
             self.thread = None
@@ -140,6 +142,21 @@ class ClockSampler:
         except OSError:
             self.proc = None
         return self
+
+    def sample_now(self):
+        """One synchronous sample (the polling thread may be starved in a short region)."""
+        if self.thread is None:
+            return
+        nv, h = self._nv, self._h
+        try:
+            try:
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            except Exception:
+                bits = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+            self.rows.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM),
+                              nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM), bits))
+        except Exception:
+            pass
 
     def __exit__(self, *a):
         if self.thread is not None:
@@ -329,6 +346,7 @@ def run_gpu(args):
         t_start.record(stream)
         for k in range(args.steps):
             step(launch_ev[k])
+            clk.sample_now()
         t_end.record(stream)
         torch.cuda.synchronize()
         barrier()
@@ -343,26 +361,37 @@ def run_gpu(args):
     peak, peak_kind = load_peaks()
 
     # ---- e2e through the public API with host buffers ----
+    # Every step copies its own x and y in from pinned host memory, runs the
+    # SpMVs and copies its y back.  Steps alternate between two streams with
+    # their own device and host buffers, so one step's copies overlap the
+    # previous step's kernels (what a caller streaming requests does).
     x_host = torch.from_numpy(M.x_vector(csr.ncols, 0)).pin_memory()
-    y_host = torch.zeros(csr.nrows, dtype=torch.float64).pin_memory()
-    xd = torch.empty_like(x)
-    yd = torch.empty_like(y)
+    e2e_streams = [torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)]
+    e2e_bufs = [(torch.empty_like(x), torch.empty_like(y),
+                 torch.zeros(csr.nrows, dtype=torch.float64).pin_memory(),
+                 torch.zeros(csr.nrows, dtype=torch.float64).pin_memory()) for _ in range(2)]
 
-    def e2e_step():
-        xd.copy_(x_host, non_blocking=True)
-        yd.copy_(y_host, non_blocking=True)
-        for r, m in mats:
-            S.SPC5_Spmv(m, xd, yd)
-        y_host.copy_(yd, non_blocking=True)
+    def e2e_step(k):
+        xd, yd, yh_in, yh_out = e2e_bufs[k % 2]
+        with torch.cuda.stream(e2e_streams[k % 2]):
+            xd.copy_(x_host, non_blocking=True)
+            yd.copy_(yh_in, non_blocking=True)
+            for r, m in mats:
+                S.SPC5_Spmv(m, xd, yd)
+            yh_out.copy_(yd, non_blocking=True)
 
-    for _ in range(max(1, args.warmup)):
-        e2e_step()
+    for k in range(max(1, args.warmup)):
+        e2e_step(k)
     torch.cuda.synchronize()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.steps):
-        e2e_step()
+    for st in e2e_streams:
+        st.wait_event(e0)
+    for k in range(args.steps):
+        e2e_step(k)
+    for st in e2e_streams:
+        stream.wait_stream(st)
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))

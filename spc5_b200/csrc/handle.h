@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <memory>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -123,10 +124,25 @@ struct SpmvPart {
     int nsplit = 0;
 };
 
-// A copy of the matrix with its block-rows sorted by size (plan.cu).
+// A copy of the matrix with its block-rows sorted by size (plan.cu).  Its
+// parts write disjoint rows of y, so an SpMV forks them onto two streams of
+// the plan and joins them back to the caller's stream.
 struct SortedPlan {
     Owned sbrptr, sheaders, svalues, svalptr, perm;
     std::vector<SpmvPart> parts;
+    cudaStream_t aux[2] = {nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
+    std::mutex mu;  // one fork/join at a time (the events are shared)
+    SortedPlan() = default;
+    SortedPlan(const SortedPlan&) = delete;
+    SortedPlan& operator=(const SortedPlan&) = delete;
+    ~SortedPlan() {
+        for (auto& st : aux)
+            if (st) cudaStreamDestroy(st);
+        if (fork) cudaEventDestroy(fork);
+        for (auto& e : join)
+            if (e) cudaEventDestroy(e);
+    }
     long bytes() const {
         long n = long(sbrptr.bytes + sheaders.bytes + svalues.bytes + svalptr.bytes + perm.bytes);
         for (const auto& p : parts) n += long(p.split.bytes);

@@ -184,6 +184,9 @@ void build_sorted_plan(spc5cuda_mat* m, cudaStream_t s) {
         part.split.alloc(sizeof(int) * size_t(part.nsplit + 1));
         launch_partition_range(part.a, part.b, plan->sbrptr.as<int>(), part.nsplit, part.split.as<int>(), s);
     }
+    for (auto& st : plan->aux) SPC5_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    SPC5_CUDA(cudaEventCreateWithFlags(&plan->fork, cudaEventDisableTiming));
+    for (auto& e : plan->join) SPC5_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     SPC5_CUDA(cudaStreamSynchronize(s));
     m->plan = std::move(plan);
 }
@@ -211,15 +214,35 @@ BetaView plan_view(const spc5cuda_mat* m, const SpmvPart& part) {
 }
 
 void plan_spmv(const spc5cuda_mat* m, const void* x, void* y, bool mixed, cudaStream_t s) {
-    for (const auto& part : m->plan->parts) {
+    SortedPlan& p = *m->plan;
+    // the parts write disjoint rows of y: the group-kernel part runs on one
+    // plan stream, the smaller row-kernel parts on the other, the largest
+    // row-kernel part on the caller's stream; all start after the work
+    // already queued on s and s waits for all of them
+    std::lock_guard<std::mutex> lk(p.mu);
+    SPC5_CUDA(cudaEventRecord(p.fork, s));
+    for (auto st : p.aux) SPC5_CUDA(cudaStreamWaitEvent(st, p.fork, 0));
+    int biggest = -1;
+    long most = -1;
+    for (size_t i = 0; i < p.parts.size(); ++i) {
+        const long blocks = p.parts[i].lanes ? long(p.parts[i].b - p.parts[i].a) : -1;
+        if (blocks > most) most = blocks, biggest = int(i);
+    }
+    for (size_t i = 0; i < p.parts.size(); ++i) {
+        const auto& part = p.parts[i];
+        cudaStream_t st = part.lanes == 0 ? p.aux[0] : (int(i) == biggest ? s : p.aux[1]);
         // the launchers pick the row kernel when the view has warp ranges
         const BetaView v = plan_view(m, part);
         if (m->value_type == SPC5CUDA_F64)
-            launch_spmv_f64(v, static_cast<const double*>(x), static_cast<double*>(y), s);
+            launch_spmv_f64(v, static_cast<const double*>(x), static_cast<double*>(y), st);
         else if (mixed)
-            launch_spmv_mixed(v, static_cast<const float*>(x), static_cast<double*>(y), s);
+            launch_spmv_mixed(v, static_cast<const float*>(x), static_cast<double*>(y), st);
         else
-            launch_spmv_f32(v, static_cast<const float*>(x), static_cast<float*>(y), s);
+            launch_spmv_f32(v, static_cast<const float*>(x), static_cast<float*>(y), st);
+    }
+    for (int k = 0; k < 2; ++k) {
+        SPC5_CUDA(cudaEventRecord(p.join[k], p.aux[k]));
+        SPC5_CUDA(cudaStreamWaitEvent(s, p.join[k], 0));
     }
 }
 
