@@ -192,8 +192,9 @@ SPC5CUDA_API spc5cuda_status spc5cuda_mat_info(const spc5cuda_mat* mat, spc5cuda
  *             it.  AUTO uses it when some block-row does not fit the row
  *             kernel (power-law and other irregular matrices).
  * spc5cuda_mat_kernel reports the kernel SpMV uses now (GROUPS, ROWS or
- * SORTED; AUTO before conversion).  Selecting SORTED on a converted matrix
- * builds the sorted copy and synchronises the device. */
+ * SORTED; AUTO before conversion).  Selecting SORTED (or AUTO, where it picks
+ * the plan) on a converted matrix builds the sorted copy; selecting GROUPS or
+ * ROWS releases it.  Both synchronise the device. */
 #define SPC5CUDA_KERNEL_AUTO 0
 #define SPC5CUDA_KERNEL_GROUPS 1
 #define SPC5CUDA_KERNEL_ROWS 2

@@ -276,8 +276,11 @@ spc5cuda_status spc5cuda_mat_set_kernel(spc5cuda_mat* m, int kernel) {
         if (kernel == SPC5CUDA_KERNEL_ROWS && m->r != 0)
             require(m->rows_ok, SPC5CUDA_ERR_UNSUPPORTED, "a block-row exceeds the row kernel's buffers");
         m->kernel = kernel;
-        if (m->r != 0 && m->wants_plan() && !m->plan) {
-            build_sorted_plan(m, nullptr);
+        if (m->r != 0 && m->wants_plan() && !m->plan) build_sorted_plan(m, nullptr);
+        // the group and row kernels run on the handle's own arrays: release the copy
+        if (kernel == SPC5CUDA_KERNEL_GROUPS || kernel == SPC5CUDA_KERNEL_ROWS) {
+            if (m->plan) SPC5_CUDA(cudaDeviceSynchronize());  // no SpMV may still read it
+            m->plan.reset();
         }
     });
 }

@@ -213,8 +213,10 @@ def test_kernel_selection(cuda):
     pl = converted(M.powerlaw(20000, seed=7), np.float64, 2)
     assert pl.kernel == S.KERNEL_SORTED
     before = pl.info().device_bytes
-    pl.set_kernel(S.KERNEL_GROUPS)
-    assert pl.kernel == S.KERNEL_GROUPS and pl.info().device_bytes == before  # the copy stays
+    pl.set_kernel(S.KERNEL_GROUPS)  # releases the sorted copy
+    assert pl.kernel == S.KERNEL_GROUPS and pl.info().device_bytes < before
+    pl.set_kernel(S.KERNEL_AUTO)  # builds it again
+    assert pl.kernel == S.KERNEL_SORTED and pl.info().device_bytes == before
 
 
 @pytest.mark.parametrize("r", [1, 2, 4, 8])
