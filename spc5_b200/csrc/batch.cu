@@ -4,10 +4,13 @@
 // Every matrix is cut into jobs of about kJobBlocks blocks along block-row
 // boundaries; each pass of kc right-hand sides (kc a power of two, at most
 // the register budget of its r) is a separate job.  Jobs are grouped by
-// (value kind, r, kc): one launch of the batched SpMM kernel per class walks
-// its job list with a fixed grid.  The class launches are captured as
-// parallel branches of one graph, so small matrices of different classes
-// share the GPU; spc5cuda_batch_launch replays the graph.
+// (value kind, r, kc, kernel): one launch of the batched SpMM kernel per class
+// walks its job list with a fixed grid.  Matrices whose every block-row fits
+// the row kernels' staging buffers (and that did not ask for the group
+// kernel) run the staged SpMM, one warp per job; the others the group SpMM.
+// The class launches are captured as parallel branches of one graph, so small
+// matrices of different classes share the GPU; spc5cuda_batch_launch replays
+// the graph.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -51,8 +54,8 @@ spc5cuda_status spc5cuda_batch_create(spc5cuda_batch** out, int n, spc5cuda_mat*
         auto* bt = new spc5cuda_batch();
         try {
             std::vector<BatchMat> hm(static_cast<size_t>(n));
-            // class (kind, r, kc) -> jobs
-            std::map<std::tuple<int, int, int>, std::vector<BatchJob>> classes;
+            // class (kind, r, kc, staged) -> jobs
+            std::map<std::tuple<int, int, int, bool>, std::vector<BatchJob>> classes;
             for (int i = 0; i < n; ++i) {
                 const spc5cuda_mat* m = mats[i];
                 require(m && m->r != 0, SPC5CUDA_ERR_FORMAT, "batch matrices must be converted");
@@ -90,8 +93,10 @@ spc5cuda_status spc5cuda_batch_create(spc5cuda_batch** out, int n, spc5cuda_mat*
                 }
                 int kofs = 0;
                 while (kofs < k[i]) {
-                    const int kc = batch_kc(m->r, k[i] - kofs);
-                    auto& list = classes[std::make_tuple(kind, m->r, kc)];
+                    const bool staged = m->spmm_view().wstart != nullptr;
+                    const int kc = staged ? spmm_rows_kc(vs_of(m->value_type), m->r, k[i] - kofs)
+                                          : batch_kc(m->r, k[i] - kofs);
+                    auto& list = classes[std::make_tuple(kind, m->r, kc, staged)];
                     for (auto& pc : pieces) list.push_back(BatchJob{i, pc.first, pc.second, kofs});
                     kofs += kc;
                 }
@@ -129,12 +134,17 @@ spc5cuda_status spc5cuda_batch_create(spc5cuda_batch** out, int n, spc5cuda_mat*
             const int sms = sm_count();
             for (auto& kv : classes) {
                 const int kind = std::get<0>(kv.first), r = std::get<1>(kv.first), kc = std::get<2>(kv.first);
+                const bool staged = std::get<3>(kv.first);
                 const int vs = kind == 0 ? 8 : 16;
                 const int njobs = int(kv.second.size());
                 const int ctas = std::max(1, std::min(div_up(long(njobs) * vs, 128), sms * 16));
                 SPC5_CUDA(cudaStreamWaitEvent(br[c], fork, 0));
-                launch_batch(kind, r, kc, bt->mats.as<BatchMat>(), bt->jobs[c].as<BatchJob>(), njobs,
-                             ctas, br[c]);
+                if (staged)
+                    launch_batch_rows(kind, r, kc, bt->mats.as<BatchMat>(), bt->jobs[c].as<BatchJob>(), njobs,
+                                      br[c]);
+                else
+                    launch_batch(kind, r, kc, bt->mats.as<BatchMat>(), bt->jobs[c].as<BatchJob>(), njobs,
+                                 ctas, br[c]);
                 SPC5_CUDA(cudaEventRecord(done[c], br[c]));
                 SPC5_CUDA(cudaStreamWaitEvent(cap, done[c], 0));
                 ++c;

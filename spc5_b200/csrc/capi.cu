@@ -407,10 +407,10 @@ spc5cuda_status spc5cuda_spmm(const spc5cuda_mat* m, int k, const void* X, long 
         require(X && Y, SPC5CUDA_ERR_INVALID, "null block of vectors");
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         if (m->value_type == SPC5CUDA_F64)
-            launch_spmm_f64(m->view(), k, static_cast<const double*>(X), ldx, 1,
+            launch_spmm_f64(m->spmm_view(), k, static_cast<const double*>(X), ldx, 1,
                             static_cast<double*>(Y), ldy, 1, s);
         else
-            launch_spmm_f32(m->view(), k, static_cast<const float*>(X), ldx, 1,
+            launch_spmm_f32(m->spmm_view(), k, static_cast<const float*>(X), ldx, 1,
                             static_cast<float*>(Y), ldy, 1, s);
     });
 }
@@ -425,7 +425,7 @@ spc5cuda_status spc5cuda_spmm_mixed(const spc5cuda_mat* m, int k, const float* X
         require(k >= 0 && ldx >= k && ldy >= k, SPC5CUDA_ERR_INVALID, "k / leading dimensions");
         if (m->nrows == 0 || k == 0) return;
         require(X && Y, SPC5CUDA_ERR_INVALID, "null block of vectors");
-        launch_spmm_mixed(m->view(), k, X, ldx, 1, Y, ldy, 1, static_cast<cudaStream_t>(stream));
+        launch_spmm_mixed(m->spmm_view(), k, X, ldx, 1, Y, ldy, 1, static_cast<cudaStream_t>(stream));
     });
 }
 

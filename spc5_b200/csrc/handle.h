@@ -202,6 +202,19 @@ struct spc5cuda_mat {
         }
         return v;
     }
+    // The view of the SpMM kernels: the per-warp ranges of the staged kernel
+    // whenever every block-row fits its buffers, unless the group kernel was
+    // requested.
+    BetaView spmm_view() const {
+        BetaView v = view();
+        v.wstart = nullptr;
+        v.nwarps = 0;
+        if (rows_ok && nwarps > 0 && kernel != SPC5CUDA_KERNEL_GROUPS) {
+            v.wstart = wstart.as<int>();
+            v.nwarps = nwarps;
+        }
+        return v;
+    }
     // The thread-per-sub-row kernel runs when every block-row fits its
     // staging buffers: on request, or by default for r <= 4 (at r = 8 every
     // block costs eight lanes a header decode each, and the group kernel is

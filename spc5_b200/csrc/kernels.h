@@ -97,6 +97,16 @@ void launch_spmm_f32(const BetaView& m, int k, const float* x, long ldx, long xc
 void launch_spmm_mixed(const BetaView& m, int k, const float* x, long ldx, long xcs, double* y,
                        long ldy, long ycs, cudaStream_t s);
 
+// ---- staged SpMM (spmm_rows.cu) over the per-warp ranges m.wstart /
+// m.nwarps of a matrix whose block-rows fit the row kernels' buffers; same
+// arguments and results as launch_spmm_*.
+void launch_spmm_rows_f64(const BetaView& m, int k, const double* x, long ldx, long xcs, double* y,
+                          long ldy, long ycs, cudaStream_t s);
+void launch_spmm_rows_f32(const BetaView& m, int k, const float* x, long ldx, long xcs, float* y,
+                          long ldy, long ycs, cudaStream_t s);
+void launch_spmm_rows_mixed(const BetaView& m, int k, const float* x, long ldx, long xcs, double* y,
+                            long ldy, long ycs, cudaStream_t s);
+
 // ---- batched SpMM (spmm.cu): many matrices, one launch per (r, kc) class
 struct BatchMat {
     const int* brptr;
@@ -123,5 +133,12 @@ int batch_kc(int r, int k);
 // kind 0 = f64, 1 = f32, 2 = mixed (f32 values and x, f64 y)
 void launch_batch(int kind, int r, int kc, const BatchMat* mats, const BatchJob* jobs, int njobs,
                   int ctas, cudaStream_t s);
+// Right-hand sides per pass of the staged SpMM for VS columns per block,
+// rows-per-block r and k right-hand sides left.
+int spmm_rows_kc(int vs, int r, int k);
+// The same for matrices whose block-rows fit the row kernels' buffers
+// (spmm_rows.cu): one warp per job at a time; kc from spmm_rows_kc.
+void launch_batch_rows(int kind, int r, int kc, const BatchMat* mats, const BatchJob* jobs, int njobs,
+                       cudaStream_t s);
 
 }  // namespace spc5cuda

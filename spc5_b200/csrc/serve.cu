@@ -8,14 +8,16 @@
 //   * whenever a slot is free and requests are pending, it takes the matrix
 //     whose oldest request waits longest, coalesces up to max_k of its
 //     requests (copies each x into a column of X), runs one multi-RHS SpMM
-//     (spmm.cu) and copies each column of Y to its request's y;
+//     (spmm.cu, spmm_rows.cu) and copies each column of Y to its request's
+//     y; a lone request runs the matrix's SpMV into its own y instead;
 //   * requests that arrive while launches are in flight wait for the next
 //     free slot and are batched then, so up to `slots` launches overlap on
 //     the device and the batch size adapts to the arrival rate;
 //   * completion is detected with an event per launch; latency is measured
 //     from submit to the host seeing the event complete.
-// Every column of the SpMM is bit-identical to a solo SpMV, so a request's
-// result does not depend on what it was batched with.
+// Every column of the SpMM is bit-identical to a solo SpMV (every SpMV kernel
+// gives the same bits), so a request's result does not depend on what it was
+// batched with.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -94,6 +96,7 @@ struct spc5cuda_server {
 
     void run();
     bool dispatch(Slot& sl);
+    bool finish_dispatch(Slot& sl, int k);
     void complete(Slot& sl);
 };
 
@@ -146,6 +149,20 @@ bool spc5cuda_server::dispatch(Slot& sl) {
         std::lock_guard<std::mutex> lk(mu);
         for (long id : sl.reqs) io.emplace_back(reqs[id].x, reqs[id].y);
     }
+    if (k == 1) {
+        // a lone request: an SpMV straight into its own y, no staging copies
+        void* y0 = io[0].second;
+        SPC5_CUDA(cudaMemsetAsync(y0, 0, size_t(m->nrows) * yb, sl.stream));
+        if (m->use_plan())
+            plan_spmv(m, io[0].first, y0, cfg.mixed, sl.stream);
+        else if (cfg.mixed)
+            launch_spmv_mixed(m->view(), static_cast<const float*>(io[0].first), static_cast<double*>(y0),
+                              sl.stream);
+        else
+            launch_spmv_f64(m->view(), static_cast<const double*>(io[0].first), static_cast<double*>(y0),
+                            sl.stream);
+        return finish_dispatch(sl, k);
+    }
     char* X = sl.X.as<char>();
     char* Y = sl.Y.as<char>();
     for (int q = 0; q < k; ++q)
@@ -153,14 +170,18 @@ bool spc5cuda_server::dispatch(Slot& sl) {
                                   cudaMemcpyDeviceToDevice, sl.stream));
     SPC5_CUDA(cudaMemsetAsync(Y, 0, size_t(k) * ldY * yb, sl.stream));
     if (cfg.mixed)
-        launch_spmm_mixed(m->view(), k, reinterpret_cast<const float*>(X), 1, ldX,
+        launch_spmm_mixed(m->spmm_view(), k, reinterpret_cast<const float*>(X), 1, ldX,
                           reinterpret_cast<double*>(Y), 1, ldY, sl.stream);
     else
-        launch_spmm_f64(m->view(), k, reinterpret_cast<const double*>(X), 1, ldX,
+        launch_spmm_f64(m->spmm_view(), k, reinterpret_cast<const double*>(X), 1, ldX,
                         reinterpret_cast<double*>(Y), 1, ldY, sl.stream);
     for (int q = 0; q < k; ++q)
         SPC5_CUDA(cudaMemcpyAsync(io[size_t(q)].second, Y + size_t(q) * ldY * yb, size_t(m->nrows) * yb,
                                   cudaMemcpyDeviceToDevice, sl.stream));
+    return finish_dispatch(sl, k);
+}
+
+bool spc5cuda_server::finish_dispatch(Slot& sl, int k) {
     SPC5_CUDA(cudaEventRecord(sl.event, sl.stream));
     sl.busy = true;
     {

@@ -251,16 +251,19 @@ void launch_spmm_impl(const BetaView& m, int k, const X* x, long ldx, long xcs, 
 
 void launch_spmm_f64(const BetaView& m, int k, const double* x, long ldx, long xcs, double* y,
                      long ldy, long ycs, cudaStream_t s) {
+    if (m.wstart) return launch_spmm_rows_f64(m, k, x, ldx, xcs, y, ldy, ycs, s);
     launch_spmm_impl<double, double, double, double, double>(m, k, x, ldx, xcs, y, ldy, ycs, s);
 }
 
 void launch_spmm_f32(const BetaView& m, int k, const float* x, long ldx, long xcs, float* y,
                      long ldy, long ycs, cudaStream_t s) {
+    if (m.wstart) return launch_spmm_rows_f32(m, k, x, ldx, xcs, y, ldy, ycs, s);
     launch_spmm_impl<float, float, float, float, float>(m, k, x, ldx, xcs, y, ldy, ycs, s);
 }
 
 void launch_spmm_mixed(const BetaView& m, int k, const float* x, long ldx, long xcs, double* y,
                        long ldy, long ycs, cudaStream_t s) {
+    if (m.wstart) return launch_spmm_rows_mixed(m, k, x, ldx, xcs, y, ldy, ycs, s);
     launch_spmm_impl<float, float, float, double, double>(m, k, x, ldx, xcs, y, ldy, ycs, s);
 }
 

@@ -28,58 +28,19 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "rows_stage.cuh"
 
 namespace spc5cuda {
 
 namespace {
 
-constexpr int ROWS_THREADS = 128;
-constexpr int ROWS_WARPS = ROWS_THREADS / 32;
+using rows::FULL;
+constexpr int ROWS_THREADS = rows::THREADS;
+constexpr int ROWS_WARPS = rows::WARPS;
 constexpr int ROWS_CTAS_PER_SM = 16;
-constexpr unsigned FULL = 0xffffffffu;
-
-__device__ __forceinline__ void cp_async16(uint32_t saddr, const void* gptr) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(gptr) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-// Waits until at most one committed group of this thread is still in flight.
-__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-
-// Bulk prefetch of [p, p + bytes) into L2 (p 16-byte aligned, bytes a
-// multiple of 16); no data is returned.
-__device__ __forceinline__ void l2_prefetch(const void* p, uint32_t bytes) {
-    if (bytes) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
-}
 
 template <class LT, int R, class V, int L>
-struct RowGeo {
-    static constexpr int VS = Layout<LT>::VS;
-    static constexpr int MB = Layout<LT>::MASK_BYTES;
-    static constexpr int STRIDE = Header<LT, R>::STRIDE;
-    static constexpr int MW = Header<LT, R>::MASK_WORDS;
-    static constexpr int LOAD_WORDS = Header<LT, R>::LOAD_WORDS;
-    static_assert(L >= R && L <= Layout<LT>::VS && 32 % L == 0, "lanes per block-row");
-    static constexpr int SPW = 32 / L;   // block-rows per chunk (L lanes each)
-    static constexpr int HB = 2048;      // header bytes per warp buffer (ROWS_HB)
-    static constexpr int VB = 8192;      // value bytes per warp buffer (ROWS_VB)
-    static constexpr int EPU = 16 / int(sizeof(V));
-    static constexpr int BUF_BYTES = HB + VB;
-    static constexpr int WARP_BYTES = BUF_BYTES;
-    static constexpr int SMEM = ROWS_WARPS * WARP_BYTES;
-};
-
-// One chunk of a warp's range: block-rows r0 .. r0 + nrow - 1 (at most
-// 32 / r), small enough for one staging buffer.  Lane k < nrow holds the end
-// block and end value of block-row r0 + k.
-struct Chunk {
-    int r0, nrow;
-    int b_lo, v_lo;  // first block and first value of the chunk
-    long h_al;       // 16-byte aligned start of the chunk's header bytes
-    int v_al;        // start of the chunk's values, rounded down to 16 bytes
-    int b_hi, v_hi;  // this lane's block-row end (lane < nrow)
-    int hunits, vunits;
-};
+using RowGeo = rows::Geo<LT, R, V, L>;
 
 template <class LT, int R, class V, class X, class A, class Y, int L>
 __global__ void __launch_bounds__(ROWS_THREADS)
@@ -88,7 +49,7 @@ __global__ void __launch_bounds__(ROWS_THREADS)
            const int* __restrict__ wstart, int nwarps, const int* __restrict__ perm,
            const X* __restrict__ x, Y* __restrict__ y) {
     using G = RowGeo<LT, R, V, L>;
-    constexpr int VS = G::VS, MB = G::MB, S = G::STRIDE, MW = G::MW, SPW = G::SPW, EPU = G::EPU;
+    constexpr int VS = G::VS, MB = G::MB, MW = G::MW;
     constexpr int FPW = 4 / MB;  // mask fields per 32-bit word
     constexpr int BITS = 8 * MB;
     constexpr uint32_t FMASK = MB == 1 ? 0xFFu : 0xFFFFu;
@@ -100,98 +61,20 @@ __global__ void __launch_bounds__(ROWS_THREADS)
     const int warp = blockIdx.x * ROWS_WARPS + wi;
     const int slot = lane / L;  // block-row of the chunk
     const int q = lane % L;     // column class: this lane owns columns c = q + L k
-    unsigned char* wbuf = smem + wi * G::WARP_BYTES;
-    const uint32_t s_w = uint32_t(__cvta_generic_to_shared(wbuf));
 
     int r_begin = 0, r_stop = 0;
     if (warp < nwarps) {
         r_begin = __ldg(wstart + warp);
         r_stop = __ldg(wstart + warp + 1);
     }
-    if (r_begin >= r_stop) return;  // warp-uniform
-    const uint64_t pol_stream = l2_evict_first_policy();
     const uint64_t pol_x = l2_evict_last_policy();
-    // end of this warp's header bytes and values: prefetches stay inside
-    const long h_stop = (long(__ldg(brptr + r_stop)) * S + 15) & ~15L;
-    const long v_stop = (long(__ldg(valptr + r_stop)) + EPU - 1) & ~long(EPU - 1);
-
-    // ---- the chunk starting at block-row r0 (nrow = 0 past the range).
-    // bounds() issues the loads of the block-row ends (lane k: block-row
-    // r0 + k), finish() decides how many block-rows fit the buffers; the
-    // loads of the next chunk are issued a chunk ahead of their use.
-    struct Bounds {
-        int r0, b_lo, v_lo, b_hi, v_hi;
-        bool cand;
-    };
-    auto bounds = [&](int r0, int b_lo, int v_lo) {
-        Bounds bd;
-        bd.r0 = r0;
-        bd.b_lo = b_lo;
-        bd.v_lo = v_lo;
-        bd.cand = lane < SPW && r0 + lane < r_stop;
-        bd.b_hi = bd.cand ? __ldg(brptr + r0 + lane + 1) : 0;
-        bd.v_hi = bd.cand ? __ldg(valptr + r0 + lane + 1) : 0;
-        return bd;
-    };
-    auto finish = [&](const Bounds& bd) {
-        Chunk ch;
-        ch.r0 = bd.r0;
-        ch.b_lo = bd.b_lo;
-        ch.v_lo = bd.v_lo;
-        ch.b_hi = bd.b_hi;
-        ch.v_hi = bd.v_hi;
-        ch.h_al = (long(ch.b_lo) * S) & ~15L;
-        ch.v_al = ch.v_lo & ~(EPU - 1);
-        bool fits = false;
-        if (bd.cand) {
-            const long hneed = ((long(ch.b_hi) * S + 15) & ~15L) - ch.h_al;
-            const long vneed = long((ch.v_hi + EPU - 1) & ~(EPU - 1)) - ch.v_al;
-            fits = hneed <= G::HB && vneed * long(sizeof(V)) <= G::VB;
-        }
-        // the ends grow with the lane, so the fitting lanes are a prefix; the
-        // host admits only matrices whose every block-row fits alone
-        ch.nrow = __popc(__ballot_sync(FULL, fits));
-        const int last = ch.nrow > 0 ? ch.nrow - 1 : 0;
-        const int b_end = __shfl_sync(FULL, ch.b_hi, last);
-        const int v_end = __shfl_sync(FULL, ch.v_hi, last);
-        ch.hunits = 0;
-        ch.vunits = 0;
-        if (ch.nrow > 0) {
-            ch.hunits = int((((long(b_end) * S + 15) & ~15L) - ch.h_al) >> 4);
-            ch.vunits = (v_end - ch.v_al + EPU - 1) / EPU;
-        }
-        return ch;
-    };
-
-    // ---- copy a chunk's headers and values into buffer bi (one commit group)
-    auto stage = [&](const Chunk& ch, int bi) {
-        const uint32_t s_h = s_w + uint32_t(bi * G::BUF_BYTES);
-        const uint32_t s_v = s_h + uint32_t(G::HB);
-        const uint8_t* hsrc = headers + ch.h_al;
-        for (int u = lane; u < ch.hunits; u += 32) cp_async16_hint(s_h + 16u * uint32_t(u), hsrc + 16L * u, pol_stream);
-        const V* vsrc = values + ch.v_al;
-        for (int u = lane; u < ch.vunits; u += 32) cp_async16_hint(s_v + 16u * uint32_t(u), vsrc + long(u) * EPU, pol_stream);
-        cp_async_commit();
-        // warm L2 with the data after this chunk (the next one is about as
-        // large), clipped to this warp's range
-        if (lane == 0 && ch.nrow > 0 && ch.r0 + ch.nrow < r_stop) {
-            const long h0 = ch.h_al + 16L * ch.hunits;
-            const long hn = std::min(16L * ch.hunits, h_stop - h0);
-            if (hn > 0) l2_prefetch(headers + h0, uint32_t(hn));
-            const long v0 = long(ch.v_al) + long(ch.vunits) * EPU;
-            const long vn = std::min(long(ch.vunits) * EPU, v_stop - v0);
-            if (vn > 0) l2_prefetch(values + v0, uint32_t(vn * long(sizeof(V))));
-        }
-    };
 
     // ---- sub-row `sub` of block-row r0 + slot of a staged chunk
-    auto compute = [&](const Chunk& ch, int bi) {
+    auto compute = [&](const rows::Chunk& ch, const uint32_t* hw, const V* vbuf) {
         constexpr int CPL = VS / L;  // columns per lane
         // blocks per step: the x loads of all of them are issued before the
         // FMAs, which still run block by block (the chain order is kept)
         constexpr int U = (16 / CPL) < 1 ? 1 : ((16 / CPL) > 8 ? 8 : 16 / CPL);
-        const uint32_t* hw = reinterpret_cast<const uint32_t*>(wbuf + bi * G::BUF_BYTES);
-        const V* vbuf = reinterpret_cast<const V*>(wbuf + bi * G::BUF_BYTES + G::HB);
         const int src = slot > 0 ? slot - 1 : 0;
         const int b_prev = __shfl_sync(FULL, ch.b_hi, src);
         const int v_prev = __shfl_sync(FULL, ch.v_hi, src);
@@ -200,26 +83,6 @@ __global__ void __launch_bounds__(ROWS_THREADS)
         int b = mine ? (slot > 0 ? b_prev : ch.b_lo) : 0;
         const int b_stop = mine ? b_mine : 0;
         int v = (mine ? (slot > 0 ? v_prev : ch.v_lo) : 0) - ch.v_al;  // buffer index of the block's values
-
-        // Header of block bb from the staged records: column and the mask
-        // words (mask of sub-row i in field i % FPW of word i / FPW).
-        auto decode = [&](int bb, int& col, uint32_t (&mw)[MW]) {
-            const long off = long(bb) * S - ch.h_al;
-            uint32_t lw[G::LOAD_WORDS + 1];
-#pragma unroll
-            for (int w = 0; w < G::LOAD_WORDS; ++w) lw[w] = hw[(off >> 2) + w];
-            lw[G::LOAD_WORDS] = 0u;
-            if constexpr (S % 4 == 0) {
-                col = int(lw[0]);
-#pragma unroll
-                for (int w = 0; w < MW; ++w) mw[w] = lw[1 + w];
-            } else {
-                const unsigned sh = unsigned(off & 3) * 8u;
-                col = int(__funnelshift_r(lw[0], lw[1], sh));
-                mw[0] = __funnelshift_r(lw[1], lw[2], sh) &
-                        ((1u << (8 * Header<LT, R>::MASK_BYTES_TOTAL)) - 1u);
-            }
-        };
 
         A acc[R][CPL];
 #pragma unroll
@@ -235,17 +98,13 @@ __global__ void __launch_bounds__(ROWS_THREADS)
                 col[u] = 0;
 #pragma unroll
                 for (int w = 0; w < MW; ++w) mw[u][w] = 0u;
-                if (b + u < b_stop) decode(b + u, col[u], mw[u]);
+                if (b + u < b_stop) col[u] = rows::decode_staged<LT, R>(hw, long(b + u) * G::STRIDE - ch.h_al, mw[u]);
             }
             // x of this lane's columns where some sub-row has a value
             X xk[U][CPL];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                uint32_t uni = 0;
-#pragma unroll
-                for (int w = 0; w < MW; ++w) uni |= mw[u][w];
-                if constexpr (MB == 1) uni = (uni | (uni >> 16)) | ((uni | (uni >> 16)) >> 8);
-                else uni = uni | (uni >> 16);
+                const uint32_t uni = rows::mask_union<LT, R>(mw[u]);
                 const X* xp = x + col[u] + q;
 #pragma unroll
                 for (int k = 0; k < CPL; ++k)
@@ -253,32 +112,8 @@ __global__ void __launch_bounds__(ROWS_THREADS)
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                // per mask word: exclusive prefix of the sub-row value counts,
-                // one field per sub-row
                 uint32_t pre[MW];
-                int tot = 0;
-                {
-                    uint32_t carry = 0;
-#pragma unroll
-                    for (int w = 0; w < MW; ++w) {
-                        uint32_t cnt;
-                        if constexpr (MB == 1) {
-                            cnt = mw[u][w] - ((mw[u][w] >> 1) & 0x55555555u);
-                            cnt = (cnt & 0x33333333u) + ((cnt >> 2) & 0x33333333u);
-                            cnt = (cnt + (cnt >> 4)) & 0x0F0F0F0Fu;
-                            pre[w] = cnt * 0x01010100u + carry * 0x01010101u;
-                            carry += (cnt * 0x01010101u) >> 24;
-                        } else {
-                            cnt = mw[u][w] - ((mw[u][w] >> 1) & 0x55555555u);
-                            cnt = (cnt & 0x33333333u) + ((cnt >> 2) & 0x33333333u);
-                            cnt = (cnt + (cnt >> 4)) & 0x0F0F0F0Fu;
-                            cnt = (cnt + (cnt >> 8)) & 0x001F001Fu;
-                            pre[w] = (cnt << 16) + carry * 0x00010001u;
-                            carry += (cnt + (cnt >> 16)) & 0xFFFFu;
-                        }
-                    }
-                    tot = int(carry);
-                }
+                const int tot = rows::subrow_prefix<LT, R>(mw[u], pre);
 #pragma unroll
                 for (int k = 0; k < CPL; ++k) {
                     const int c = q + L * k;
@@ -286,21 +121,7 @@ __global__ void __launch_bounds__(ROWS_THREADS)
 #pragma unroll
                     for (int w = 0; w < MW; ++w) {
                         // field i: buffer offset of sub-row i's value in column c
-                        uint32_t off;
-                        if constexpr (R == 1) {
-                            off = uint32_t(__popc(mw[u][0] & below));
-                        } else if constexpr (MB == 1) {
-                            uint32_t t = mw[u][w] & (below * 0x01010101u);
-                            t = t - ((t >> 1) & 0x55555555u);
-                            t = (t & 0x33333333u) + ((t >> 2) & 0x33333333u);
-                            off = pre[w] + ((t + (t >> 4)) & 0x0F0F0F0Fu);
-                        } else {
-                            uint32_t t = mw[u][w] & (below * 0x00010001u);
-                            t = t - ((t >> 1) & 0x55555555u);
-                            t = (t & 0x33333333u) + ((t >> 2) & 0x33333333u);
-                            t = (t + (t >> 4)) & 0x0F0F0F0Fu;
-                            off = pre[w] + ((t + (t >> 8)) & 0x001F001Fu);
-                        }
+                        const uint32_t off = rows::column_offsets<LT, R>(mw[u][w], pre[w], below);
 #pragma unroll
                         for (int f = 0; f < FPW; ++f) {
                             const int i = w * FPW + f;
@@ -341,21 +162,7 @@ __global__ void __launch_bounds__(ROWS_THREADS)
         }
     };
 
-    // ---- walk the range: copy a chunk, load the next chunk's bounds while
-    // the copies fly, compute, repeat
-    Chunk cur = finish(bounds(r_begin, __ldg(brptr + r_begin), __ldg(valptr + r_begin)));
-    while (cur.nrow > 0) {  // warp-uniform
-        stage(cur, 0);
-        const int last = cur.nrow - 1;
-        const int r_next = cur.r0 + cur.nrow;
-        const Bounds nb = bounds(r_next, __shfl_sync(FULL, cur.b_hi, last), __shfl_sync(FULL, cur.v_hi, last));
-        cp_async_wait_all();
-        __syncwarp();
-        compute(cur, 0);
-        __syncwarp();  // the next chunk overwrites the buffer
-        cur = r_next < r_stop ? finish(nb) : Chunk{r_next, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    }
-    cp_async_wait_all();
+    rows::walk<LT, R, V, L>(brptr, headers, values, valptr, r_begin, r_stop, smem + wi * G::BUF_BYTES, compute);
 }
 
 template <class K>
@@ -462,8 +269,8 @@ int rows_warps(int vs, int r, int lanes) {
 }
 
 // Staging buffer sizes of RowGeo (every instantiation).
-constexpr int ROWS_HB = 2048;
-constexpr int ROWS_VB = 8192;
+constexpr int ROWS_HB = rows::HB;
+constexpr int ROWS_VB = rows::VB;
 
 bool rows_fit(int vs, int r, int max_blocks, int max_values) {
     // every block-row alone must fit the staging buffers, alignment included

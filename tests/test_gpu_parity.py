@@ -312,6 +312,41 @@ def test_spmm_columns_equal_spmv(cuda, tag, dt, r, k):
             assert Y[:, j].tobytes() == yj.tobytes(), (csr.name, j)
 
 
+@pytest.mark.parametrize("tag,dt", DTYPES + [("mixed", np.float32)])
+@pytest.mark.parametrize("r", [1, 2, 4, 8])
+def test_spmm_staged_and_group_bit_exact(cuda, tag, dt, r):
+    """The staged SpMM (matrices whose block-rows fit the row kernels'
+    buffers) and the group SpMM (KERNEL_GROUPS, or block-rows too large) give
+    the oracle's SpMV bits in every column, for k = 1, 5 (passes of 4 + 1) and
+    16, with row-major X and Y of padded leading dimension."""
+    mixed = tag == "mixed"
+    f = oracle.beta_spmv_mixed if mixed else (oracle.beta_spmv_f64 if dt == np.float64 else oracle.beta_spmv_f32)
+    ydt = np.float64 if mixed else dt
+    for csr in kernel_cases():
+        if csr.nnz > 400_000:
+            continue
+        for kernel in (S.KERNEL_AUTO, S.KERNEL_GROUPS):
+            m = S.csr_matrix(csr.rowptr, csr.colidx, csr.values.astype(dt), csr.ncols)
+            m.set_kernel(kernel)
+            S.CSR_to_SPC5(m, S.FORMAT_OF_R[r])
+            brptr, headers, vals = m.arrays()
+            for k in (1, 5, 16):
+                X = np.zeros((csr.ncols, k + 3), dtype=dt)
+                Y0 = np.zeros((csr.nrows, k + 2), dtype=ydt)
+                for j in range(k):
+                    X[:, j] = M.x_vector(csr.ncols, 70 + j, dt)
+                    Y0[:, j] = M.x_vector(csr.nrows, 90 + j, ydt)
+                Xd, Yd = dev(X), dev(Y0)
+                (S.SPC5_Spmm_mixed if mixed else S.SPC5_Spmm)(m, Xd[:, :k], Yd[:, :k])
+                torch.cuda.synchronize()
+                Y = Yd.cpu().numpy()
+                assert Y[:, k:].tobytes() == Y0[:, k:].tobytes()  # padding untouched
+                for j in range(k):
+                    yo = f(r, csr.nrows, brptr, headers, vals, np.ascontiguousarray(X[:, j]),
+                           np.ascontiguousarray(Y0[:, j]))
+                    assert Y[:, j].tobytes() == yo.tobytes(), (csr.name, kernel, k, j)
+
+
 @pytest.mark.parametrize("r", [1, 4, 8])
 def test_spmm_mixed_columns(cuda, r):
     csr = M.powerlaw(5000, seed=12)
