@@ -665,7 +665,7 @@ TRAFFIC_RATIO = {"powerlaw": {1: 1.193, 2: 1.119, 4: 1.065, 8: 1.025},
 
 # spc5cuda_mat_kernel codes: SPC5CUDA_KERNEL_GROUPS = 1, SPC5CUDA_KERNEL_ROWS = 2
 KERNEL_NAME = {1: "k_spmv (group per block-row stream)", 2: "k_rows (thread per sub-row)",
-               3: "sorted plan (k_spmv + k_rows by block-row size)", 0: "unconverted"}
+               3: "sorted plan (k_rows by block-row size; largest block-rows in segments)", 0: "unconverted"}
 
 
 def select_kernel(m, which):

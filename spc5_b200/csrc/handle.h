@@ -116,12 +116,17 @@ inline void require(bool cond, spc5cuda_status s, const char* what) {
 // One part of the length-sorted plan: sorted block-rows [a, b), run by the
 // row kernel with `lanes` lanes per block-row (split: one range per warp), or
 // by the group kernel when lanes == 0 (split: one range per group); split
-// holds nsplit + 1 block-row starts.
+// holds nsplit + 1 block-row starts.  A segmented part (nseg = b - a > 0,
+// a = 0) holds block-rows too large to stage: cut into segments that are,
+// interleaved per warp; vbrptr / vvalptr are the segments' block and value
+// offsets and split their per-warp ranges.
 struct SpmvPart {
     int lanes = 0;
     int a = 0, b = 0;
+    int nseg = 0;
     Owned split;
     int nsplit = 0;
+    Owned vbrptr, vvalptr;
 };
 
 // A copy of the matrix with its block-rows sorted by size (plan.cu).  Its
@@ -145,7 +150,7 @@ struct SortedPlan {
     }
     long bytes() const {
         long n = long(sbrptr.bytes + sheaders.bytes + svalues.bytes + svalptr.bytes + perm.bytes);
-        for (const auto& p : parts) n += long(p.split.bytes);
+        for (const auto& p : parts) n += long(p.split.bytes + p.vbrptr.bytes + p.vvalptr.bytes);
         return n;
     }
 };

@@ -52,6 +52,9 @@ struct BetaView {
     const int* wstart = nullptr;
     int nwarps = 0;
     int lanes = 0;               // row kernel: lanes per block-row (0: r)
+    // row kernel: > 0 when these arrays hold the segments of nseg long
+    // block-rows, interleaved per warp (the sorted plan's largest part)
+    int nseg = 0;
     // block-row of y for each block-row of these arrays (null: the same);
     // set when the arrays are a reordered copy of the matrix
     const int* perm = nullptr;
@@ -79,6 +82,9 @@ bool rows_fit(int vs, int r, int max_blocks, int max_values);
 // rows_lane_units(...) <= L * rows_unit().
 long rows_lane_units(int vs, int r, int nblocks, int nvalues);
 long rows_unit();
+// Header and value bytes of one warp's staging buffer.
+int rows_hb();
+int rows_vb();
 void blockrow_max(int nbr, const int* brptr, const int* valptr, int* max_blocks, int* max_values,
                   cudaStream_t s);
 void launch_rows_f64(const BetaView& m, const double* x, double* y, cudaStream_t s);

@@ -7,10 +7,12 @@
 // accumulator sees the same FMA chain and y is bit-identical -- plus perm[i],
 // the block-row of y that sorted block-row i belongs to.  The sorted order is
 // cut into parts, each run by the kernel that suits its block-rows:
-//   * block-rows too large for the row kernel's chunks: the group kernel, on
-//     a balanced split of the part (neighbouring block-rows now have about
-//     the same size, so the groups of a warp stay in step and rarely end a
-//     row inside a window);
+//   * block-rows too large for the row kernel's chunks: cut into segments
+//     of at most L/32 of a chunk's buffers (greedy, in block order), the
+//     segments of 32 / L neighbouring block-rows interleaved so that a chunk
+//     holds segment k of each of them; the row kernel (L lanes per
+//     block-row) then stages them like short block-rows while every lane
+//     keeps its block-row's accumulators from chunk to chunk;
 //   * the rest: the row kernel with L = 8, 4, 2 or 1 lanes per block-row,
 //     the smallest L whose chunk of 32 / L block-rows fits the staging
 //     buffers.  Block-rows of one chunk have about the same size, so no lane
@@ -81,7 +83,171 @@ __global__ void k_class_counts(int nbr, const unsigned long long* __restrict__ s
     }
 }
 
+// Values of block b (popcount of its mask bytes).
+__device__ __forceinline__ int block_values(const uint8_t* __restrict__ hdr, long b, int stride) {
+    int n = 0;
+    for (int k = 4; k < stride; ++k) n += __popc(unsigned(hdr[b * stride + k]));
+    return n;
+}
+
+// Greedy cut of blocks [b0, b1) (first value v0) into segments of at most
+// bmax blocks and vmax values, in block order: emit(k, first block, blocks,
+// first value, values) for segment k.
+template <class F>
+__device__ void cut_segments(int b0, int b1, int v0, const uint8_t* __restrict__ hdr, int stride, int bmax,
+                             int vmax, F&& emit) {
+    int k = 0, sb = b0, sv = v0, nb = 0, nv = 0;
+    for (int b = b0; b < b1; ++b) {
+        const int pc = block_values(hdr, b, stride);
+        if (nb > 0 && (nb + 1 > bmax || nv + pc > vmax)) {
+            emit(k++, sb, nb, sv, nv);
+            sb = b;
+            sv += nv;
+            nb = 0;
+            nv = 0;
+        }
+        ++nb;
+        nv += pc;
+    }
+    if (nb > 0) emit(k, sb, nb, sv, nv);
+}
+
+// nseg_of[i] = segments of sorted block-row i < nlong.
+__global__ void k_seg_count(int nlong, const int* __restrict__ sbrptr, const int* __restrict__ svalptr,
+                            const uint8_t* __restrict__ hdr, int stride, int bmax, int vmax,
+                            int* __restrict__ nseg_of) {
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nlong; i += long(gridDim.x) * blockDim.x) {
+        int n = 0;
+        cut_segments(sbrptr[i], sbrptr[i + 1], svalptr[i], hdr, stride, bmax, vmax,
+                     [&](int, int, int, int, int) { ++n; });
+        nseg_of[i] = n;
+    }
+}
+
+// Segment rows of warp g: (most segments of its block-rows) x (its block-rows).
+__global__ void k_seg_warp_rows(int nlong, int spw, int nw, const int* __restrict__ nseg_of,
+                                int* __restrict__ vrows) {
+    for (long g = long(blockIdx.x) * blockDim.x + threadIdx.x; g < nw; g += long(gridDim.x) * blockDim.x) {
+        const int a = int(g) * spw, n = min(spw, nlong - a);
+        int most = 0;
+        for (int s = 0; s < n; ++s) most = max(most, nseg_of[a + s]);
+        vrows[g] = most * n;
+    }
+}
+
+// Segment k of block-row i (warp g = i / spw, slot s = i % spw) is segment
+// row wbase[g] + k n_g + s: its block and value counts (vnb, vnv, zero for
+// the rows of block-rows with fewer segments) and where it starts in the
+// sorted copy (vsb, vsv).
+__global__ void k_seg_fill(int nlong, int spw, const int* __restrict__ sbrptr, const int* __restrict__ svalptr,
+                           const uint8_t* __restrict__ hdr, int stride, int bmax, int vmax,
+                           const int* __restrict__ wbase, int* __restrict__ vnb, int* __restrict__ vnv,
+                           int* __restrict__ vsb, int* __restrict__ vsv) {
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nlong; i += long(gridDim.x) * blockDim.x) {
+        const int g = int(i) / spw, s = int(i) % spw;
+        const int n = min(spw, nlong - g * spw);
+        const int base = wbase[g];
+        cut_segments(sbrptr[i], sbrptr[i + 1], svalptr[i], hdr, stride, bmax, vmax,
+                     [&](int k, int sb, int nb, int sv, int nv) {
+                         const long v = base + long(k) * n + s;
+                         vnb[v] = nb;
+                         vnv[v] = nv;
+                         vsb[v] = sb;
+                         vsv[v] = sv;
+                     });
+    }
+}
+
+// Copy every segment row to its place (one warp per segment row).
+template <class V>
+__global__ void k_seg_copy(int nv, const int* __restrict__ vsb, const int* __restrict__ vsv,
+                           const int* __restrict__ vbrptr, const int* __restrict__ vvalptr, int stride,
+                           const uint8_t* __restrict__ hdr, uint8_t* __restrict__ thdr, const V* __restrict__ vals,
+                           V* __restrict__ tvals) {
+    const int lane = threadIdx.x & 31;
+    const long warps = long(gridDim.x) * blockDim.x / 32;
+    for (long v = (long(blockIdx.x) * blockDim.x + threadIdx.x) / 32; v < nv; v += warps) {
+        const long nb = vbrptr[v + 1] - vbrptr[v];
+        if (nb == 0) continue;
+        const long h0 = long(vsb[v]) * stride, d0 = long(vbrptr[v]) * stride, hn = nb * stride;
+        for (long k = lane; k < hn; k += 32) thdr[d0 + k] = hdr[h0 + k];
+        const long w0 = vsv[v], e0 = vvalptr[v], en = long(vvalptr[v + 1]) - e0;
+        for (long k = lane; k < en; k += 32) tvals[e0 + k] = vals[w0 + k];
+    }
+}
+
 int grid_for(long n, int threads) { return std::max(1, std::min(div_up(n, threads), sm_count() * 8)); }
+
+}  // namespace
+
+namespace {
+
+// Cuts the part's block-rows (sorted positions [0, nseg)) into segments of
+// at most 1/32 of a chunk's buffers per lane, rewrites that region of the
+// sorted copy in the interleaved segment order and builds the part's segment
+// offsets and per-warp ranges (synchronises s).
+void build_segments(const spc5cuda_mat* m, SortedPlan* plan, SpmvPart& part, int stride, int vbytes,
+                    cudaStream_t s) {
+    const int nlong = part.nseg;
+    const int L = part.lanes;
+    const int spw = 32 / L;
+    // the budget of a block-row that L lanes stage in one chunk
+    const int bmax = int(L * (rows_hb() - 32) / 32 / stride);
+    const int vmax = int(L * (rows_vb() - 32) / 32 / vbytes);
+    const int nw = (nlong + spw - 1) / spw;
+    const int* sbrptr = plan->sbrptr.as<int>();
+    const int* svalptr = plan->svalptr.as<int>();
+    DevBuf nseg_of(sizeof(int) * size_t(nlong), s), vrows(sizeof(int) * size_t(nw), s);
+    k_seg_count<<<grid_for(nlong, 128), 128, 0, s>>>(nlong, sbrptr, svalptr, plan->sheaders.as<uint8_t>(), stride,
+                                                     bmax, vmax, nseg_of.as<int>());
+    SPC5_CUDA(cudaGetLastError());
+    k_seg_warp_rows<<<grid_for(nw, 128), 128, 0, s>>>(nlong, spw, nw, nseg_of.as<int>(), vrows.as<int>());
+    SPC5_CUDA(cudaGetLastError());
+    part.split.alloc(sizeof(int) * size_t(nw + 1));
+    part.nsplit = nw;
+    {
+        DevBuf tmp(sizeof(int) * size_t(scan_tmp_ints(nw)), s);
+        exclusive_scan_i32(vrows.as<int>(), part.split.as<int>(), nw, tmp.as<int>(), s);
+    }
+    int nv = 0;
+    SPC5_CUDA(cudaMemcpyAsync(&nv, part.split.as<int>() + nw, sizeof(int), cudaMemcpyDeviceToHost, s));
+    int ends[2] = {0, 0};  // blocks and values of the part
+    SPC5_CUDA(cudaMemcpyAsync(&ends[0], sbrptr + nlong, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SPC5_CUDA(cudaMemcpyAsync(&ends[1], svalptr + nlong, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SPC5_CUDA(cudaStreamSynchronize(s));
+    DevBuf vnb(sizeof(int) * size_t(nv), s), vnv(sizeof(int) * size_t(nv), s);
+    DevBuf vsb(sizeof(int) * size_t(nv), s), vsv(sizeof(int) * size_t(nv), s);
+    SPC5_CUDA(cudaMemsetAsync(vnb.p, 0, vnb.bytes, s));
+    SPC5_CUDA(cudaMemsetAsync(vnv.p, 0, vnv.bytes, s));
+    k_seg_fill<<<grid_for(nlong, 128), 128, 0, s>>>(nlong, spw, sbrptr, svalptr, plan->sheaders.as<uint8_t>(),
+                                                    stride, bmax, vmax, part.split.as<int>(), vnb.as<int>(),
+                                                    vnv.as<int>(), vsb.as<int>(), vsv.as<int>());
+    SPC5_CUDA(cudaGetLastError());
+    part.vbrptr.alloc(sizeof(int) * size_t(nv + 1));
+    part.vvalptr.alloc(sizeof(int) * size_t(nv + 1));
+    {
+        DevBuf tmp(sizeof(int) * size_t(scan_tmp_ints(nv)), s);
+        exclusive_scan_i32(vnb.as<int>(), part.vbrptr.as<int>(), nv, tmp.as<int>(), s);
+        exclusive_scan_i32(vnv.as<int>(), part.vvalptr.as<int>(), nv, tmp.as<int>(), s);
+    }
+    // the segments hold exactly the part's blocks and values: rewrite that
+    // region of the sorted copy in segment order
+    const size_t hbytes = size_t(ends[0]) * size_t(stride), vbytes_all = size_t(ends[1]) * size_t(vbytes);
+    DevBuf th(std::max<size_t>(16, hbytes), s), tv(std::max<size_t>(16, vbytes_all), s);
+    const int blocks = std::max(1, std::min(div_up(long(nv) * 32, 256), sm_count() * 16));
+    if (m->value_type == SPC5CUDA_F64)
+        k_seg_copy<double><<<blocks, 256, 0, s>>>(nv, vsb.as<int>(), vsv.as<int>(), part.vbrptr.as<int>(),
+                                                  part.vvalptr.as<int>(), stride, plan->sheaders.as<uint8_t>(),
+                                                  th.as<uint8_t>(), plan->svalues.as<double>(), tv.as<double>());
+    else
+        k_seg_copy<float><<<blocks, 256, 0, s>>>(nv, vsb.as<int>(), vsv.as<int>(), part.vbrptr.as<int>(),
+                                                 part.vvalptr.as<int>(), stride, plan->sheaders.as<uint8_t>(),
+                                                 th.as<uint8_t>(), plan->svalues.as<float>(), tv.as<float>());
+    SPC5_CUDA(cudaGetLastError());
+    if (hbytes) SPC5_CUDA(cudaMemcpyAsync(plan->sheaders.p, th.p, hbytes, cudaMemcpyDeviceToDevice, s));
+    if (vbytes_all) SPC5_CUDA(cudaMemcpyAsync(plan->svalues.p, tv.p, vbytes_all, cudaMemcpyDeviceToDevice, s));
+    SPC5_CUDA(cudaStreamSynchronize(s));
+}
 
 }  // namespace
 
@@ -159,7 +325,17 @@ void build_sorted_plan(spc5cuda_mat* m, cudaStream_t s) {
     // boundary is at least the previous one (sizes descend)
     const int above8 = counts[0];
     int lo = above8;
-    if (above8 > 0) plan->parts.push_back({0, 0, above8});
+    if (above8 > 0) {
+        SpmvPart seg;
+        // lanes per block-row of the segments (measured on B200, power-law
+        // N = 4M: more lanes give longer segments and more warps, fewer
+        // give more block-rows per warp instruction)
+        seg.lanes = r == 1 ? 4 : (r == 2 ? 8 : r);
+        seg.a = 0;
+        seg.b = above8;
+        seg.nseg = above8;
+        plan->parts.push_back(std::move(seg));
+    }
     const int lanes_of[4] = {8, 4, 2, 1};
     for (int j = 0; j < 4; ++j) {
         const int L = lanes_of[j];
@@ -175,6 +351,10 @@ void build_sorted_plan(spc5cuda_mat* m, cudaStream_t s) {
     // ---- a balanced split of every part
     for (auto& part : plan->parts) {
         const int rows = part.b - part.a;
+        if (part.nseg > 0) {
+            build_segments(m, plan.get(), part, stride, vbytes, s);
+            continue;
+        }
         if (part.lanes == 0) {
             part.nsplit = std::max(1, std::min(spmv_groups(vs, r), rows));
         } else {
@@ -202,6 +382,11 @@ BetaView plan_view(const spc5cuda_mat* m, const SpmvPart& part) {
     v.values = p.svalues.p;
     v.valptr = p.svalptr.as<int>();
     v.perm = p.perm.as<int>();
+    if (part.nseg > 0) {
+        v.brptr = part.vbrptr.as<int>();
+        v.valptr = part.vvalptr.as<int>();
+        v.nseg = part.nseg;
+    }
     if (part.lanes == 0) {
         v.gstart = part.split.as<int>();
         v.ngroups = part.nsplit;
@@ -215,22 +400,22 @@ BetaView plan_view(const spc5cuda_mat* m, const SpmvPart& part) {
 
 void plan_spmv(const spc5cuda_mat* m, const void* x, void* y, bool mixed, cudaStream_t s) {
     SortedPlan& p = *m->plan;
-    // the parts write disjoint rows of y: the group-kernel part runs on one
-    // plan stream, the smaller row-kernel parts on the other, the largest
-    // row-kernel part on the caller's stream; all start after the work
-    // already queued on s and s waits for all of them
+    // the parts write disjoint rows of y: the segmented part (the largest
+    // block-rows) runs on one plan stream, the smaller row-kernel parts on
+    // the other, the largest of those on the caller's stream; all start
+    // after the work already queued on s and s waits for all of them
     std::lock_guard<std::mutex> lk(p.mu);
     SPC5_CUDA(cudaEventRecord(p.fork, s));
     for (auto st : p.aux) SPC5_CUDA(cudaStreamWaitEvent(st, p.fork, 0));
     int biggest = -1;
     long most = -1;
     for (size_t i = 0; i < p.parts.size(); ++i) {
-        const long blocks = p.parts[i].lanes ? long(p.parts[i].b - p.parts[i].a) : -1;
+        const long blocks = (p.parts[i].lanes && !p.parts[i].nseg) ? long(p.parts[i].b - p.parts[i].a) : -1;
         if (blocks > most) most = blocks, biggest = int(i);
     }
     for (size_t i = 0; i < p.parts.size(); ++i) {
         const auto& part = p.parts[i];
-        cudaStream_t st = part.lanes == 0 ? p.aux[0] : (int(i) == biggest ? s : p.aux[1]);
+        cudaStream_t st = (part.lanes == 0 || part.nseg) ? p.aux[0] : (int(i) == biggest ? s : p.aux[1]);
         // the launchers pick the row kernel when the view has warp ranges
         const BetaView v = plan_view(m, part);
         if (m->value_type == SPC5CUDA_F64)

@@ -61,14 +61,16 @@ struct Chunk {
 
 // Walks block-rows [r_begin, r_stop) of one matrix (warp-uniform bounds):
 // stage a chunk into wbuf, load the next chunk's bounds while the copies fly,
-// call compute(chunk, staged header words, staged values), repeat.  The
+// call compute(chunk, staged header words, staged values), repeat.  A chunk
+// holds at most `cap` (<= 32 / L) block-rows: as many as fit the buffer.  The
 // caller guarantees that every block-row alone fits the buffer.
 template <class LT, int R, class V, int L, class F>
 __device__ __forceinline__ void walk(const int* __restrict__ brptr, const uint8_t* __restrict__ headers,
                                      const V* __restrict__ values, const int* __restrict__ valptr,
-                                     int r_begin, int r_stop, unsigned char* wbuf, F&& compute) {
+                                     int r_begin, int r_stop, unsigned char* wbuf, F&& compute,
+                                     int cap = 32 / L) {
     using G = Geo<LT, R, V, L>;
-    constexpr int S = G::STRIDE, SPW = G::SPW, EPU = G::EPU;
+    constexpr int S = G::STRIDE, EPU = G::EPU;
     if (r_begin >= r_stop) return;
     const int lane = threadIdx.x & 31;
     const uint32_t s_h = uint32_t(__cvta_generic_to_shared(wbuf));
@@ -91,7 +93,7 @@ __device__ __forceinline__ void walk(const int* __restrict__ brptr, const uint8_
         bd.r0 = r0;
         bd.b_lo = b_lo;
         bd.v_lo = v_lo;
-        bd.cand = lane < SPW && r0 + lane < r_stop;
+        bd.cand = lane < cap && r0 + lane < r_stop;
         bd.b_hi = bd.cand ? __ldg(brptr + r0 + lane + 1) : 0;
         bd.v_hi = bd.cand ? __ldg(valptr + r0 + lane + 1) : 0;
         return bd;

@@ -42,18 +42,26 @@ constexpr int ROWS_CTAS_PER_SM = 16;
 template <class LT, int R, class V, int L>
 using RowGeo = rows::Geo<LT, R, V, L>;
 
-template <class LT, int R, class V, class X, class A, class Y, int L>
+// SEG: the block-rows are segments of long block-rows (the length-sorted
+// plan's largest ones), laid out so that chunk k of warp w holds segment k of
+// each of the block-rows w * 32 / L + slot (nseg of them, ng = min(32 / L,
+// nseg - w * 32 / L) in warp w): a lane keeps its accumulators from chunk to
+// chunk and adds its row sum to y after the last one (perm[w * 32 / L +
+// slot] is the block-row of y).  The FMA chain of every (sub-row, column) is
+// the block-row's own, in block order.
+template <class LT, int R, class V, class X, class A, class Y, int L, bool SEG>
 __global__ void __launch_bounds__(ROWS_THREADS)
     k_rows(int nrows, const int* __restrict__ brptr, const uint8_t* __restrict__ headers,
            const V* __restrict__ values, const int* __restrict__ valptr,
-           const int* __restrict__ wstart, int nwarps, const int* __restrict__ perm,
+           const int* __restrict__ wstart, int nwarps, const int* __restrict__ perm, int nseg,
            const X* __restrict__ x, Y* __restrict__ y) {
     using G = RowGeo<LT, R, V, L>;
-    constexpr int VS = G::VS, MB = G::MB, MW = G::MW;
+    constexpr int VS = G::VS, MB = G::MB, MW = G::MW, SPW = G::SPW;
     constexpr int FPW = 4 / MB;  // mask fields per 32-bit word
     constexpr int BITS = 8 * MB;
     constexpr uint32_t FMASK = MB == 1 ? 0xFFu : 0xFFFFu;
     constexpr bool Y_ATOMIC = sizeof(Y) == 8;  // red.add.f64 is y + s rounded once
+    constexpr int CPL = VS / L;  // columns per lane
     extern __shared__ __align__(16) unsigned char smem[];
 
     const int lane = threadIdx.x & 31;
@@ -69,9 +77,42 @@ __global__ void __launch_bounds__(ROWS_THREADS)
     }
     const uint64_t pol_x = l2_evict_last_policy();
 
-    // ---- sub-row `sub` of block-row r0 + slot of a staged chunk
+    A acc[R][CPL];
+    auto zero = [&]() {
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+#pragma unroll
+            for (int k = 0; k < CPL; ++k) acc[i][k] = A(0);
+    };
+    // ---- row sums: the _mm512_reduce_add tree (distance VS/2, ..., 1).
+    // Levels of distance >= L pair columns of the same class inside the
+    // lane; the last log2(L) levels pair the lanes of the block-row.  Then
+    // y[brow * R + q] += sum of sub-row q (warp-uniform call).
+    auto flush = [&](bool mine, int brow) {
+        A res = A(0);
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+#pragma unroll
+            for (int d = CPL / 2; d >= 1; d >>= 1) {
+#pragma unroll
+                for (int k = 0; k < d; ++k) acc[i][k] = acc[i][k] + acc[i][k + d];
+            }
+            A sum = acc[i][0];
+#pragma unroll
+            for (int d = L / 2; d >= 1; d >>= 1) sum = sum + __shfl_xor_sync(FULL, sum, d);
+            if (i == q) res = sum;
+        }
+        if (mine && q < R) {
+            const long yrow = long(brow) * R + q;
+            if (yrow < nrows) {
+                if constexpr (Y_ATOMIC) atomicAdd(y + yrow, Y(res));
+                else y[yrow] = y[yrow] + Y(res);
+            }
+        }
+    };
+
+    // ---- the blocks of block-row r0 + slot of a staged chunk
     auto compute = [&](const rows::Chunk& ch, const uint32_t* hw, const V* vbuf) {
-        constexpr int CPL = VS / L;  // columns per lane
         // blocks per step: the x loads of all of them are issued before the
         // FMAs, which still run block by block (the chain order is kept)
         constexpr int U = (16 / CPL) < 1 ? 1 : ((16 / CPL) > 8 ? 8 : 16 / CPL);
@@ -84,12 +125,7 @@ __global__ void __launch_bounds__(ROWS_THREADS)
         const int b_stop = mine ? b_mine : 0;
         int v = (mine ? (slot > 0 ? v_prev : ch.v_lo) : 0) - ch.v_al;  // buffer index of the block's values
 
-        A acc[R][CPL];
-#pragma unroll
-        for (int i = 0; i < R; ++i)
-#pragma unroll
-            for (int k = 0; k < CPL; ++k) acc[i][k] = A(0);
-
+        if constexpr (!SEG) zero();
         while (__any_sync(FULL, b < b_stop)) {
             int col[U];
             uint32_t mw[U][MW];
@@ -136,33 +172,19 @@ __global__ void __launch_bounds__(ROWS_THREADS)
             }
             b += U;
         }
-        // ---- row sums: the _mm512_reduce_add tree (distance VS/2, ..., 1).
-        // Levels of distance >= L pair columns of the same class inside the
-        // lane; the last log2(L) levels pair the lanes of the block-row.
-        A res = A(0);
-#pragma unroll
-        for (int i = 0; i < R; ++i) {
-#pragma unroll
-            for (int d = CPL / 2; d >= 1; d >>= 1) {
-#pragma unroll
-                for (int k = 0; k < d; ++k) acc[i][k] = acc[i][k] + acc[i][k + d];
-            }
-            A sum = acc[i][0];
-#pragma unroll
-            for (int d = L / 2; d >= 1; d >>= 1) sum = sum + __shfl_xor_sync(FULL, sum, d);
-            if (i == q) res = sum;
-        }
-        if (mine && q < R) {
-            const int brow = perm ? __ldg(perm + ch.r0 + slot) : ch.r0 + slot;
-            const long yrow = long(brow) * R + q;
-            if (yrow < nrows) {
-                if constexpr (Y_ATOMIC) atomicAdd(y + yrow, Y(res));
-                else y[yrow] = y[yrow] + Y(res);
-            }
-        }
+        if constexpr (!SEG) flush(mine, mine ? (perm ? __ldg(perm + ch.r0 + slot) : ch.r0 + slot) : 0);
     };
 
-    rows::walk<LT, R, V, L>(brptr, headers, values, valptr, r_begin, r_stop, smem + wi * G::BUF_BYTES, compute);
+    unsigned char* wbuf = smem + wi * G::BUF_BYTES;
+    if constexpr (SEG) {
+        if (warp >= nwarps) return;  // warp-uniform
+        const int ng = min(SPW, nseg - warp * SPW);
+        zero();
+        rows::walk<LT, R, V, L>(brptr, headers, values, valptr, r_begin, r_stop, wbuf, compute, ng);
+        flush(slot < ng, slot < ng ? __ldg(perm + warp * SPW + slot) : 0);
+    } else {
+        rows::walk<LT, R, V, L>(brptr, headers, values, valptr, r_begin, r_stop, wbuf, compute);
+    }
 }
 
 template <class K>
@@ -214,7 +236,7 @@ int rows_occupancy(int r, int lanes) {
     dispatch_rl(r, lanes, [&](auto RC, auto LC) {
         constexpr int R_ = decltype(RC)::value, L_ = decltype(LC)::value;
         using G = RowGeo<LT, R_, V, L_>;
-        auto kern = k_rows<LT, R_, V, X, A, Y, L_>;
+        auto kern = k_rows<LT, R_, V, X, A, Y, L_, false>;
         set_smem(kern, G::SMEM);
         SPC5_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, ROWS_THREADS, G::SMEM));
     });
@@ -229,10 +251,10 @@ void launch_rows_impl(const BetaView& m, const X* x, Y* y, cudaStream_t s) {
     dispatch_rl(m.r, m.lanes, [&](auto RC, auto LC) {
         constexpr int R_ = decltype(RC)::value, L_ = decltype(LC)::value;
         using G = RowGeo<LT, R_, V, L_>;
-        auto kern = k_rows<LT, R_, V, X, A, Y, L_>;
+        auto kern = m.nseg > 0 ? k_rows<LT, R_, V, X, A, Y, L_, true> : k_rows<LT, R_, V, X, A, Y, L_, false>;
         set_smem(kern, G::SMEM);
         kern<<<ctas, ROWS_THREADS, G::SMEM, s>>>(m.nrows, m.brptr, m.headers, vals, m.valptr, m.wstart,
-                                                 m.nwarps, m.perm, x, y);
+                                                 m.nwarps, m.perm, m.nseg, x, y);
     });
     SPC5_CUDA(cudaGetLastError());
 }
@@ -290,6 +312,9 @@ long rows_lane_units(int vs, int r, int nblocks, int nvalues) {
 }
 
 long rows_unit() { return long(ROWS_HB - 32) * long(ROWS_VB - 32) / 32; }
+
+int rows_hb() { return ROWS_HB; }
+int rows_vb() { return ROWS_VB; }
 
 void blockrow_max(int nbr, const int* brptr, const int* valptr, int* max_blocks, int* max_values,
                   cudaStream_t s) {
