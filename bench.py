@@ -660,7 +660,7 @@ def run_serve(args):
 # over all launches of the call) on the same generators at smaller sizes
 # (power-law N = 1M, stencil 100^3); traffic grows with the units processed,
 # so roofline.traffic of the full workloads is these ratios times their bytes.
-TRAFFIC_RATIO = {"powerlaw": {1: 1.193, 2: 1.119, 4: 1.065, 8: 1.025},
+TRAFFIC_RATIO = {"powerlaw": {1: 1.194, 2: 1.120, 4: 1.065, 8: 1.019},
                  "stencil27": {1: 0.999, 2: 0.984, 4: 0.978, 8: 0.994}}
 
 # spc5cuda_mat_kernel codes: SPC5CUDA_KERNEL_GROUPS = 1, SPC5CUDA_KERNEL_ROWS = 2
