@@ -406,7 +406,9 @@ spc5cuda_status spc5cuda_spmm(const spc5cuda_mat* m, int k, const void* X, long 
         if (m->nrows == 0 || k == 0) return;
         require(X && Y, SPC5CUDA_ERR_INVALID, "null block of vectors");
         cudaStream_t s = static_cast<cudaStream_t>(stream);
-        if (m->value_type == SPC5CUDA_F64)
+        if (m->use_plan())
+            plan_spmm(m, k, X, ldx, 1, Y, ldy, 1, false, s);
+        else if (m->value_type == SPC5CUDA_F64)
             launch_spmm_f64(m->spmm_view(), k, static_cast<const double*>(X), ldx, 1,
                             static_cast<double*>(Y), ldy, 1, s);
         else
@@ -425,7 +427,11 @@ spc5cuda_status spc5cuda_spmm_mixed(const spc5cuda_mat* m, int k, const float* X
         require(k >= 0 && ldx >= k && ldy >= k, SPC5CUDA_ERR_INVALID, "k / leading dimensions");
         if (m->nrows == 0 || k == 0) return;
         require(X && Y, SPC5CUDA_ERR_INVALID, "null block of vectors");
-        launch_spmm_mixed(m->spmm_view(), k, X, ldx, 1, Y, ldy, 1, static_cast<cudaStream_t>(stream));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        if (m->use_plan())
+            plan_spmm(m, k, X, ldx, 1, Y, ldy, 1, true, s);
+        else
+            launch_spmm_mixed(m->spmm_view(), k, X, ldx, 1, Y, ldy, 1, s);
     });
 }
 

@@ -162,6 +162,10 @@ BetaView plan_view(const spc5cuda_mat* m, const SpmvPart& part);
 // y += A x through the plan (x, y of the handle's types; mixed: F32 handle,
 // float x, double y).
 void plan_spmv(const spc5cuda_mat* m, const void* x, void* y, bool mixed, cudaStream_t s);
+// Y += A X through the plan with the staged SpMM (element (row i, rhs q) of
+// X at x[i * ldx + q * xcs], likewise Y).
+void plan_spmm(const spc5cuda_mat* m, int k, const void* x, long ldx, long xcs, void* y, long ldy, long ycs,
+               bool mixed, cudaStream_t s);
 
 }  // namespace spc5cuda
 

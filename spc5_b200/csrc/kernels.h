@@ -82,6 +82,11 @@ bool rows_fit(int vs, int r, int max_blocks, int max_values);
 // rows_lane_units(...) <= L * rows_unit().
 long rows_lane_units(int vs, int r, int nblocks, int nvalues);
 long rows_unit();
+// Lanes per block-row of the segmented part of a sorted plan (the largest
+// block-rows), measured on B200 on the N = 4M power-law matrix: more lanes
+// give longer segments and more warps, fewer give more block-rows per warp
+// instruction.
+constexpr int seg_lanes(int r) { return r == 1 ? 4 : (r == 2 ? 8 : r); }
 // Header and value bytes of one warp's staging buffer.
 int rows_hb();
 int rows_vb();
@@ -140,8 +145,15 @@ int batch_kc(int r, int k);
 void launch_batch(int kind, int r, int kc, const BatchMat* mats, const BatchJob* jobs, int njobs,
                   int ctas, cudaStream_t s);
 // Right-hand sides per pass of the staged SpMM for VS columns per block,
-// rows-per-block r and k right-hand sides left.
-int spmm_rows_kc(int vs, int r, int k);
+// rows-per-block r and k right-hand sides left (seg: the segmented part of a
+// sorted plan, run with seg_lanes(r) lanes per block-row).
+int spmm_rows_kc(int vs, int r, int k, bool seg = false);
+// Most right-hand sides per pass of the staged SpMM with `lanes` lanes per
+// block-row: r x (vs / lanes columns per lane) x kc accumulators stay at
+// most 32, kc at most 16.
+constexpr int mm_kc_limit(int vs, int r, int lanes) {
+    return 32 / (r * (vs / lanes)) > 16 ? 16 : 32 / (r * (vs / lanes));
+}
 // The same for matrices whose block-rows fit the row kernels' buffers
 // (spmm_rows.cu): one warp per job at a time; kc from spmm_rows_kc.
 void launch_batch_rows(int kind, int r, int kc, const BatchMat* mats, const BatchJob* jobs, int njobs,

@@ -327,10 +327,7 @@ void build_sorted_plan(spc5cuda_mat* m, cudaStream_t s) {
     int lo = above8;
     if (above8 > 0) {
         SpmvPart seg;
-        // lanes per block-row of the segments (measured on B200, power-law
-        // N = 4M: more lanes give longer segments and more warps, fewer
-        // give more block-rows per warp instruction)
-        seg.lanes = r == 1 ? 4 : (r == 2 ? 8 : r);
+        seg.lanes = seg_lanes(r);
         seg.a = 0;
         seg.b = above8;
         seg.nseg = above8;
@@ -398,12 +395,16 @@ BetaView plan_view(const spc5cuda_mat* m, const SpmvPart& part) {
     return v;
 }
 
-void plan_spmv(const spc5cuda_mat* m, const void* x, void* y, bool mixed, cudaStream_t s) {
+namespace {
+
+// Runs launch(view, stream) for every part of the plan: the parts write
+// disjoint rows of y, so the segmented part (the largest block-rows) runs on
+// one plan stream, the smaller row-kernel parts on the other, the largest of
+// those on the caller's stream; all start after the work already queued on s
+// and s waits for all of them.
+template <class F>
+void run_parts(const spc5cuda_mat* m, cudaStream_t s, F&& launch) {
     SortedPlan& p = *m->plan;
-    // the parts write disjoint rows of y: the segmented part (the largest
-    // block-rows) runs on one plan stream, the smaller row-kernel parts on
-    // the other, the largest of those on the caller's stream; all start
-    // after the work already queued on s and s waits for all of them
     std::lock_guard<std::mutex> lk(p.mu);
     SPC5_CUDA(cudaEventRecord(p.fork, s));
     for (auto st : p.aux) SPC5_CUDA(cudaStreamWaitEvent(st, p.fork, 0));
@@ -416,19 +417,42 @@ void plan_spmv(const spc5cuda_mat* m, const void* x, void* y, bool mixed, cudaSt
     for (size_t i = 0; i < p.parts.size(); ++i) {
         const auto& part = p.parts[i];
         cudaStream_t st = (part.lanes == 0 || part.nseg) ? p.aux[0] : (int(i) == biggest ? s : p.aux[1]);
-        // the launchers pick the row kernel when the view has warp ranges
-        const BetaView v = plan_view(m, part);
+        launch(plan_view(m, part), st);
+    }
+    for (int k = 0; k < 2; ++k) {
+        SPC5_CUDA(cudaEventRecord(p.join[k], p.aux[k]));
+        SPC5_CUDA(cudaStreamWaitEvent(s, p.join[k], 0));
+    }
+}
+
+}  // namespace
+
+void plan_spmv(const spc5cuda_mat* m, const void* x, void* y, bool mixed, cudaStream_t s) {
+    // the launchers pick the row kernel when the view has warp ranges
+    run_parts(m, s, [&](const BetaView& v, cudaStream_t st) {
         if (m->value_type == SPC5CUDA_F64)
             launch_spmv_f64(v, static_cast<const double*>(x), static_cast<double*>(y), st);
         else if (mixed)
             launch_spmv_mixed(v, static_cast<const float*>(x), static_cast<double*>(y), st);
         else
             launch_spmv_f32(v, static_cast<const float*>(x), static_cast<float*>(y), st);
-    }
-    for (int k = 0; k < 2; ++k) {
-        SPC5_CUDA(cudaEventRecord(p.join[k], p.aux[k]));
-        SPC5_CUDA(cudaStreamWaitEvent(s, p.join[k], 0));
-    }
+    });
+}
+
+void plan_spmm(const spc5cuda_mat* m, int k, const void* x, long ldx, long xcs, void* y, long ldy, long ycs,
+               bool mixed, cudaStream_t s) {
+    run_parts(m, s, [&](const BetaView& v, cudaStream_t st) {
+        if (!v.wstart) throw Error(SPC5CUDA_ERR_INVALID, "plan part without warp ranges");
+        if (m->value_type == SPC5CUDA_F64)
+            launch_spmm_rows_f64(v, k, static_cast<const double*>(x), ldx, xcs, static_cast<double*>(y), ldy, ycs,
+                                 st);
+        else if (mixed)
+            launch_spmm_rows_mixed(v, k, static_cast<const float*>(x), ldx, xcs, static_cast<double*>(y), ldy, ycs,
+                                   st);
+        else
+            launch_spmm_rows_f32(v, k, static_cast<const float*>(x), ldx, xcs, static_cast<float*>(y), ldy, ycs,
+                                 st);
+    });
 }
 
 }  // namespace spc5cuda

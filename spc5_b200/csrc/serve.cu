@@ -169,7 +169,9 @@ bool spc5cuda_server::dispatch(Slot& sl) {
         SPC5_CUDA(cudaMemcpyAsync(X + size_t(q) * ldX * xb, io[size_t(q)].first, size_t(m->ncols) * xb,
                                   cudaMemcpyDeviceToDevice, sl.stream));
     SPC5_CUDA(cudaMemsetAsync(Y, 0, size_t(k) * ldY * yb, sl.stream));
-    if (cfg.mixed)
+    if (m->use_plan())
+        plan_spmm(m, k, X, 1, ldX, Y, 1, ldY, cfg.mixed, sl.stream);
+    else if (cfg.mixed)
         launch_spmm_mixed(m->spmm_view(), k, reinterpret_cast<const float*>(X), 1, ldX,
                           reinterpret_cast<double*>(Y), 1, ldY, sl.stream);
     else

@@ -30,32 +30,32 @@ using rows::FULL;
 
 // Lanes per block-row of the staged SpMM: one column per lane for double
 // blocks (8 columns); for float blocks (16 columns) two per lane, except at
-// r = 8 where one column per lane keeps four right-hand sides per pass.
-template <class LT, int R>
+// r = 8 where one column per lane keeps four right-hand sides per pass.  The
+// segmented part of a sorted plan keeps the plan's lanes (seg_lanes).
+template <class LT, int R, bool SEG>
 constexpr int mm_lanes() {
+    if constexpr (SEG) return seg_lanes(R);
     return (Layout<LT>::VS == 16 && R == 8) ? 16 : 8;
 }
 
-// Right-hand sides per pass: R x (columns per lane) x KC accumulators stay
-// at most 32, KC at most 16 (a power of two, the largest not above k).
-template <class LT, int R>
-constexpr int mm_kc_max() {
-    constexpr int per = 32 / (R * (Layout<LT>::VS / mm_lanes<LT, R>()));
-    return per > 16 ? 16 : per;
-}
-
 // Y += A X over block-rows [r_begin, r_stop) of one matrix for right-hand
-// sides [0, KC) of xm / ym (already offset to the pass's first one).
-template <class LT, int R, int KC, class V, class X, class A, class Y>
+// sides [0, KC) of xm / ym (already offset to the pass's first one); perm
+// (if not null) maps a block-row of these arrays to its block-row of Y.  SEG:
+// the block-rows are the interleaved segments of ng long block-rows (chunk k
+// holds segment k of each, as the segmented row kernel reads them), whose
+// block-rows of Y are perm[seg_base + slot]; a lane keeps its accumulators
+// over all chunks and Y is updated once, after the last.
+template <class LT, int R, int KC, class V, class X, class A, class Y, bool SEG>
 __device__ __forceinline__ void mm_range(int nrows, const int* __restrict__ brptr,
                                          const uint8_t* __restrict__ headers, const V* __restrict__ values,
                                          const int* __restrict__ valptr, int r_begin, int r_stop,
+                                         const int* __restrict__ perm, int ng, int seg_base,
                                          const X* __restrict__ xm, long ldx, long xcs, Y* __restrict__ ym,
                                          long ldy, long ycs, unsigned char* wbuf) {
     constexpr int VS = Layout<LT>::VS;
-    constexpr int L = mm_lanes<LT, R>();  // lanes per block-row
-    constexpr int CPL = VS / L;        // columns per lane: q + L k
-    constexpr int LOGL = L == 16 ? 4 : (L == 8 ? 3 : (L == 4 ? 2 : 1));
+    constexpr int L = mm_lanes<LT, R, SEG>();  // lanes per block-row
+    constexpr int CPL = VS / L;                // columns per lane: q + L k
+    constexpr int LOGL = L == 16 ? 4 : (L == 8 ? 3 : (L == 4 ? 2 : (L == 2 ? 1 : 0)));
     using G = rows::Geo<LT, R, V, L>;
     constexpr int MB = G::MB, MW = G::MW;
     constexpr int FPW = 4 / MB;  // mask fields per 32-bit word
@@ -72,6 +72,80 @@ __device__ __forceinline__ void mm_range(int nrows, const int* __restrict__ brpt
     const int q = lane % L;     // this lane's columns: q + L k
     const uint64_t pol_x = l2_evict_last_policy();
 
+    A acc[R][CPL][KC];
+    auto zero = [&]() {
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+#pragma unroll
+            for (int k = 0; k < CPL; ++k)
+#pragma unroll
+                for (int j = 0; j < KC; ++j) acc[i][k][j] = A(0);
+    };
+
+    // ---- row sums: the _mm512_reduce_add tree (distance VS/2, ..., 1).
+    // Levels of distance >= L pair columns of one lane.  The last log2(L)
+    // levels pair the lanes of the block-row as a reduce-scatter of the
+    // N = R KC sums: at distance d the lane with bit d set keeps the odd
+    // entries and its partner the even ones, each adding the partner's
+    // copy (the same pairs as the tree, so the same bits), until one sum
+    // per entry is left; then the plain butterfly.  Lane q ends with the
+    // entries t L + rev(q) (rev: q's log2(L) bits reversed), or, when
+    // N < L, entry rev(q) mod N in the lanes whose low bits are zero.
+    // Entries are ordered so that one store covers neighbouring
+    // addresses: (i, j) at i KC + j for row-major Y (ycs == 1), at j R + i
+    // otherwise (the R rows of consecutive block-rows are adjacent).  Then
+    // Y[brow R + i][j] += sum (warp-uniform call).
+    auto flush = [&](bool mine, int brow) {
+        constexpr int N = R * KC;
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+#pragma unroll
+            for (int j = 0; j < KC; ++j) {
+#pragma unroll
+                for (int d = CPL / 2; d >= 1; d >>= 1) {
+#pragma unroll
+                    for (int k = 0; k < d; ++k) acc[i][k][j] = acc[i][k][j] + acc[i][k + d][j];
+                }
+            }
+        }
+        const bool row_major = ycs == 1;
+        A sv[N];
+#pragma unroll
+        for (int e = 0; e < N; ++e) sv[e] = row_major ? acc[e / KC][0][e % KC] : acc[e % R][0][e / R];
+#pragma unroll
+        for (int lev = 0; lev < LOGL; ++lev) {
+            const int d = L >> (lev + 1);
+            const int n = N >> lev;  // entries still held
+            const bool hi = (q & d) != 0;
+            if (n >= 2) {
+#pragma unroll
+                for (int t = 0; t < n / 2; ++t) {
+                    const A keep = hi ? sv[2 * t + 1] : sv[2 * t];
+                    const A send = hi ? sv[2 * t] : sv[2 * t + 1];
+                    sv[t] = keep + __shfl_xor_sync(FULL, send, d);
+                }
+            } else {
+                sv[0] = sv[0] + __shfl_xor_sync(FULL, sv[0], d);
+            }
+        }
+        const int rq = LOGL ? int(__brev(unsigned(q)) >> (32 - LOGL)) : 0;
+        constexpr int PER = N >= L ? N / L : 1;
+        const bool writer = mine && (N >= L || (q & (L / N - 1)) == 0);
+        const long row0 = long(brow) * R;
+#pragma unroll
+        for (int t = 0; t < PER; ++t) {
+            const int e = N >= L ? t * L + rq : (rq & (N - 1));
+            const int i = row_major ? e / KC : e % R;
+            const int j = row_major ? e % KC : e / R;
+            const long yrow = row0 + i;
+            if (writer && yrow < nrows) {
+                Y* dst = ym + yrow * ldy + long(j) * ycs;
+                if constexpr (Y_ATOMIC) atomicAdd(dst, Y(sv[t]));
+                else *dst = *dst + Y(sv[t]);
+            }
+        }
+    };
+
     auto compute = [&](const rows::Chunk& ch, const uint32_t* hw, const V* vbuf) {
         const int src = slot > 0 ? slot - 1 : 0;
         const int b_prev = __shfl_sync(FULL, ch.b_hi, src);
@@ -82,14 +156,7 @@ __device__ __forceinline__ void mm_range(int nrows, const int* __restrict__ brpt
         const int b_stop = mine ? b_mine : 0;
         int v = (mine ? (slot > 0 ? v_prev : ch.v_lo) : 0) - ch.v_al;
 
-        A acc[R][CPL][KC];
-#pragma unroll
-        for (int i = 0; i < R; ++i)
-#pragma unroll
-            for (int k = 0; k < CPL; ++k)
-#pragma unroll
-                for (int j = 0; j < KC; ++j) acc[i][k][j] = A(0);
-
+        if constexpr (!SEG) zero();
         while (__any_sync(FULL, b < b_stop)) {
             int col[U];
             uint32_t mw[U][MW];
@@ -139,88 +206,35 @@ __device__ __forceinline__ void mm_range(int nrows, const int* __restrict__ brpt
             }
             b += U;
         }
-        // ---- row sums: the _mm512_reduce_add tree (distance VS/2, ..., 1).
-        // Levels of distance >= L pair columns of one lane.  The last log2(L)
-        // levels pair the lanes of the block-row as a reduce-scatter of the
-        // N = R KC sums: at distance d the lane with bit d set keeps the odd
-        // entries and its partner the even ones, each adding the partner's
-        // copy (the same pairs as the tree, so the same bits), until one sum
-        // per entry is left; then the plain butterfly.  Lane q ends with the
-        // entries t L + rev(q) (rev: q's log2(L) bits reversed), or, when
-        // N < L, entry rev(q) mod N in the lanes whose low bits are zero.
-        // Entries are ordered so that one store covers neighbouring
-        // addresses: (i, j) at i KC + j for row-major Y (ycs == 1), at j R + i
-        // otherwise (the R rows of consecutive block-rows are adjacent).
-        constexpr int N = R * KC;
-#pragma unroll
-        for (int i = 0; i < R; ++i) {
-#pragma unroll
-            for (int j = 0; j < KC; ++j) {
-#pragma unroll
-                for (int d = CPL / 2; d >= 1; d >>= 1) {
-#pragma unroll
-                    for (int k = 0; k < d; ++k) acc[i][k][j] = acc[i][k][j] + acc[i][k + d][j];
-                }
-            }
-        }
-        const bool row_major = ycs == 1;
-        A sv[N];
-#pragma unroll
-        for (int e = 0; e < N; ++e) sv[e] = row_major ? acc[e / KC][0][e % KC] : acc[e % R][0][e / R];
-#pragma unroll
-        for (int lev = 0; lev < LOGL; ++lev) {
-            const int d = L >> (lev + 1);
-            const int n = N >> lev;  // entries still held
-            const bool hi = (q & d) != 0;
-            if (n >= 2) {
-#pragma unroll
-                for (int t = 0; t < n / 2; ++t) {
-                    const A keep = hi ? sv[2 * t + 1] : sv[2 * t];
-                    const A send = hi ? sv[2 * t] : sv[2 * t + 1];
-                    sv[t] = keep + __shfl_xor_sync(FULL, send, d);
-                }
-            } else {
-                sv[0] = sv[0] + __shfl_xor_sync(FULL, sv[0], d);
-            }
-        }
-        const int rq = int(__brev(unsigned(q)) >> (32 - LOGL));
-        constexpr int PER = N >= L ? N / L : 1;
-        const bool writer = mine && (N >= L || (q & (L / N - 1)) == 0);
-        const long row0 = long(ch.r0 + slot) * R;
-#pragma unroll
-        for (int t = 0; t < PER; ++t) {
-            const int e = N >= L ? t * L + rq : (rq & (N - 1));
-            const int i = row_major ? e / KC : e % R;
-            const int j = row_major ? e % KC : e / R;
-            const long yrow = row0 + i;
-            if (writer && yrow < nrows) {
-                Y* dst = ym + yrow * ldy + long(j) * ycs;
-                if constexpr (Y_ATOMIC) atomicAdd(dst, Y(sv[t]));
-                else *dst = *dst + Y(sv[t]);
-            }
-        }
+        if constexpr (!SEG) flush(mine, mine ? (perm ? __ldg(perm + ch.r0 + slot) : ch.r0 + slot) : 0);
     };
-    rows::walk<LT, R, V, L>(brptr, headers, values, valptr, r_begin, r_stop, wbuf, compute);
+    if constexpr (SEG) {
+        zero();
+        rows::walk<LT, R, V, L>(brptr, headers, values, valptr, r_begin, r_stop, wbuf, compute, ng);
+        flush(slot < ng, slot < ng ? __ldg(perm + seg_base + slot) : 0);
+    } else {
+        rows::walk<LT, R, V, L>(brptr, headers, values, valptr, r_begin, r_stop, wbuf, compute);
+    }
 }
 
-// One matrix: warp w owns block-rows [wstart[w], wstart[w + 1]).
-template <class LT, int R, int KC, class V, class X, class A, class Y>
+// One matrix: warp w owns block-rows [wstart[w], wstart[w + 1]).  SEG: warp
+// w owns the segments of long block-rows w * 32 / L + slot (nseg in all).
+template <class LT, int R, int KC, class V, class X, class A, class Y, bool SEG>
 __global__ void __launch_bounds__(rows::THREADS)
     k_spmm_rows(int nrows, const int* __restrict__ brptr, const uint8_t* __restrict__ headers,
                 const V* __restrict__ values, const int* __restrict__ valptr, const int* __restrict__ wstart,
-                int nwarps, const X* __restrict__ xm, long ldx, long xcs, Y* __restrict__ ym, long ldy,
-                long ycs) {
-    using G = rows::Geo<LT, R, V, mm_lanes<LT, R>()>;
+                int nwarps, const int* __restrict__ perm, int nseg, const X* __restrict__ xm, long ldx, long xcs,
+                Y* __restrict__ ym, long ldy, long ycs) {
+    constexpr int L = mm_lanes<LT, R, SEG>();
+    using G = rows::Geo<LT, R, V, L>;
     extern __shared__ __align__(16) unsigned char smem[];
     const int wi = threadIdx.x >> 5;
     const int warp = blockIdx.x * rows::WARPS + wi;
-    int r_begin = 0, r_stop = 0;
-    if (warp < nwarps) {
-        r_begin = __ldg(wstart + warp);
-        r_stop = __ldg(wstart + warp + 1);
-    }
-    mm_range<LT, R, KC, V, X, A, Y>(nrows, brptr, headers, values, valptr, r_begin, r_stop, xm, ldx, xcs, ym,
-                                    ldy, ycs, smem + wi * G::BUF_BYTES);
+    if (warp >= nwarps) return;  // warp-uniform
+    const int r_begin = __ldg(wstart + warp), r_stop = __ldg(wstart + warp + 1);
+    const int ng = SEG ? min(G::SPW, nseg - warp * G::SPW) : 0;
+    mm_range<LT, R, KC, V, X, A, Y, SEG>(nrows, brptr, headers, values, valptr, r_begin, r_stop, perm, ng,
+                                         warp * G::SPW, xm, ldx, xcs, ym, ldy, ycs, smem + wi * G::BUF_BYTES);
 }
 
 // Batched: warps walk the job list with the grid's warp count as stride; job
@@ -229,16 +243,18 @@ __global__ void __launch_bounds__(rows::THREADS)
 template <class LT, int R, int KC, class V, class X, class A, class Y>
 __global__ void __launch_bounds__(rows::THREADS)
     k_spmm_rows_batch(const BatchMat* __restrict__ mats, const BatchJob* __restrict__ jobs, int njobs) {
-    using G = rows::Geo<LT, R, V, mm_lanes<LT, R>()>;
+    using G = rows::Geo<LT, R, V, mm_lanes<LT, R, false>()>;
     extern __shared__ __align__(16) unsigned char smem[];
     const int wi = threadIdx.x >> 5;
     const int nw = gridDim.x * rows::WARPS;
     for (int j = blockIdx.x * rows::WARPS + wi; j < njobs; j += nw) {  // warp-uniform
         const BatchJob job = jobs[j];
         const BatchMat& m = mats[job.mat];
-        mm_range<LT, R, KC, V, X, A, Y>(m.nrows, m.brptr, m.headers, static_cast<const V*>(m.values), m.valptr,
-                                        job.r_begin, job.r_end, static_cast<const X*>(m.x) + job.kofs, m.ldx, 1L,
-                                        static_cast<Y*>(m.y) + job.kofs, m.ldy, 1L, smem + wi * G::BUF_BYTES);
+        mm_range<LT, R, KC, V, X, A, Y, false>(m.nrows, m.brptr, m.headers, static_cast<const V*>(m.values),
+                                               m.valptr, job.r_begin, job.r_end, nullptr, 0, 0,
+                                               static_cast<const X*>(m.x) + job.kofs, m.ldx, 1L,
+                                               static_cast<Y*>(m.y) + job.kofs, m.ldy, 1L,
+                                               smem + wi * G::BUF_BYTES);
     }
 }
 
@@ -248,13 +264,13 @@ void set_smem(K kernel, int bytes) {
 }
 
 // Calls f(integral_constant<R>, integral_constant<KC>) for r in {1, 2, 4, 8}
-// and kc a power of two up to mm_kc_max<LT, r>().
-template <class LT, class F>
+// and kc a power of two up to mm_kc_limit of the kernel's lanes.
+template <class LT, bool SEG, class F>
 void dispatch_rkc(int r, int kc, F&& f) {
     using std::integral_constant;
     auto with_r = [&](auto RC) {
         constexpr int R_ = decltype(RC)::value;
-        constexpr int KMAX = mm_kc_max<LT, R_>();
+        constexpr int KMAX = mm_kc_limit(Layout<LT>::VS, R_, mm_lanes<LT, R_, SEG>());
         switch (kc) {
             case 1: f(RC, integral_constant<int, 1>{}); return true;
             case 2: if constexpr (KMAX >= 2) { f(RC, integral_constant<int, 2>{}); return true; } break;
@@ -274,24 +290,35 @@ void dispatch_rkc(int r, int kc, F&& f) {
     if (!done) throw Error(SPC5CUDA_ERR_INVALID, "unsupported (r, right-hand sides per pass)");
 }
 
+template <class LT, bool SEG, class V, class X, class A, class Y>
+void spmm_rows_run(const BetaView& m, int k, const X* x, long ldx, long xcs, Y* y, long ldy, long ycs,
+                   cudaStream_t s) {
+    const int ctas = (m.nwarps + rows::WARPS - 1) / rows::WARPS;
+    const V* vals = static_cast<const V*>(m.values);
+    for (int k0 = 0; k0 < k;) {
+        const int kc = spmm_rows_kc(Layout<LT>::VS, m.r, k - k0, SEG);
+        dispatch_rkc<LT, SEG>(m.r, kc, [&](auto RC, auto KCC) {
+            constexpr int R_ = decltype(RC)::value, KC_ = decltype(KCC)::value;
+            constexpr int SMEM = rows::Geo<LT, R_, V, mm_lanes<LT, R_, SEG>()>::SMEM;
+            auto kern = k_spmm_rows<LT, R_, KC_, V, X, A, Y, SEG>;
+            set_smem(kern, SMEM);
+            kern<<<ctas, rows::THREADS, SMEM, s>>>(m.nrows, m.brptr, m.headers, vals, m.valptr, m.wstart,
+                                                   m.nwarps, m.perm, m.nseg, x + long(k0) * xcs, ldx, xcs,
+                                                   y + long(k0) * ycs, ldy, ycs);
+        });
+        k0 += kc;
+    }
+}
+
 template <class LT, class V, class X, class A, class Y>
 void spmm_rows_impl(const BetaView& m, int k, const X* x, long ldx, long xcs, Y* y, long ldy, long ycs,
                     cudaStream_t s) {
     if (m.nbr <= 0 || k <= 0 || m.nwarps <= 0) return;
-    const int ctas = (m.nwarps + rows::WARPS - 1) / rows::WARPS;
-    const V* vals = static_cast<const V*>(m.values);
-    for (int k0 = 0; k0 < k;) {
-        const int kc = spmm_rows_kc(Layout<LT>::VS, m.r, k - k0);
-        dispatch_rkc<LT>(m.r, kc, [&](auto RC, auto KCC) {
-            constexpr int R_ = decltype(RC)::value, KC_ = decltype(KCC)::value;
-            constexpr int SMEM = rows::Geo<LT, R_, V, mm_lanes<LT, R_>()>::SMEM;
-            auto kern = k_spmm_rows<LT, R_, KC_, V, X, A, Y>;
-            set_smem(kern, SMEM);
-            kern<<<ctas, rows::THREADS, SMEM, s>>>(m.nrows, m.brptr, m.headers, vals, m.valptr, m.wstart,
-                                                   m.nwarps, x + long(k0) * xcs, ldx, xcs, y + long(k0) * ycs,
-                                                   ldy, ycs);
-        });
-        k0 += kc;
+    if (m.nseg > 0) {
+        if (m.lanes != seg_lanes(m.r)) throw Error(SPC5CUDA_ERR_INVALID, "segment lanes");
+        spmm_rows_run<LT, true, V, X, A, Y>(m, k, x, ldx, xcs, y, ldy, ycs, s);
+    } else {
+        spmm_rows_run<LT, false, V, X, A, Y>(m, k, x, ldx, xcs, y, ldy, ycs, s);
     }
     SPC5_CUDA(cudaGetLastError());
 }
@@ -299,9 +326,9 @@ void spmm_rows_impl(const BetaView& m, int k, const X* x, long ldx, long xcs, Y*
 template <class LT, class V, class X, class A, class Y>
 void batch_rows_impl(int r, int kc, const BatchMat* mats, const BatchJob* jobs, int njobs, int ctas,
                      cudaStream_t s) {
-    dispatch_rkc<LT>(r, kc, [&](auto RC, auto KCC) {
+    dispatch_rkc<LT, false>(r, kc, [&](auto RC, auto KCC) {
         constexpr int R_ = decltype(RC)::value, KC_ = decltype(KCC)::value;
-        constexpr int SMEM = rows::Geo<LT, R_, V, mm_lanes<LT, R_>()>::SMEM;
+        constexpr int SMEM = rows::Geo<LT, R_, V, mm_lanes<LT, R_, false>()>::SMEM;
         auto kern = k_spmm_rows_batch<LT, R_, KC_, V, X, A, Y>;
         set_smem(kern, SMEM);
         int per_sm = 0;
@@ -313,10 +340,9 @@ void batch_rows_impl(int r, int kc, const BatchMat* mats, const BatchJob* jobs, 
 
 }  // namespace
 
-int spmm_rows_kc(int vs, int r, int k) {
-    // mm_kc_max of the instantiations
-    const int kmax = vs == 8 ? (r == 1 ? 16 : r == 2 ? 16 : r == 4 ? 8 : 4)
-                             : (r == 1 ? 16 : r == 2 ? 8 : 4);
+int spmm_rows_kc(int vs, int r, int k, bool seg) {
+    const int lanes = seg ? seg_lanes(r) : ((vs == 16 && r == 8) ? 16 : 8);
+    const int kmax = mm_kc_limit(vs, r, lanes);
     int kc = 1;
     while (kc * 2 <= k && kc * 2 <= kmax) kc *= 2;
     return kc;

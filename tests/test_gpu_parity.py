@@ -316,16 +316,18 @@ def test_spmm_columns_equal_spmv(cuda, tag, dt, r, k):
 @pytest.mark.parametrize("r", [1, 2, 4, 8])
 def test_spmm_staged_and_group_bit_exact(cuda, tag, dt, r):
     """The staged SpMM (matrices whose block-rows fit the row kernels'
-    buffers) and the group SpMM (KERNEL_GROUPS, or block-rows too large) give
-    the oracle's SpMV bits in every column, for k = 1, 5 (passes of 4 + 1) and
-    16, with row-major X and Y of padded leading dimension."""
+    buffers), the group SpMM (KERNEL_GROUPS) and the staged SpMM over the
+    length-sorted plan (KERNEL_SORTED, and AUTO for block-rows too large,
+    whose largest block-rows run in segments) give the oracle's SpMV bits in
+    every column, for k = 1, 5 (passes of 4 + 1) and 16, with row-major X and
+    Y of padded leading dimension."""
     mixed = tag == "mixed"
     f = oracle.beta_spmv_mixed if mixed else (oracle.beta_spmv_f64 if dt == np.float64 else oracle.beta_spmv_f32)
     ydt = np.float64 if mixed else dt
     for csr in kernel_cases():
         if csr.nnz > 400_000:
             continue
-        for kernel in (S.KERNEL_AUTO, S.KERNEL_GROUPS):
+        for kernel in (S.KERNEL_AUTO, S.KERNEL_GROUPS, S.KERNEL_SORTED):
             m = S.csr_matrix(csr.rowptr, csr.colidx, csr.values.astype(dt), csr.ncols)
             m.set_kernel(kernel)
             S.CSR_to_SPC5(m, S.FORMAT_OF_R[r])
