@@ -231,8 +231,12 @@ SPC5CUDA_API spc5cuda_status spc5cuda_spmv_mixed(const spc5cuda_mat* mat, const 
  * right-hand sides.  X is row-major ncols x k with leading dimension
  * ldx >= k (the k values of one matrix column are contiguous), Y row-major
  * nrows x k with ldy >= k.  Column j of Y is bit-identical to spc5cuda_spmv
- * with column j of X.  k <= 16 runs in one pass over the matrix for r <= 2
- * (8 for r = 4, 4 for r = 8); larger k runs several passes. */
+ * with column j of X.  The kernel follows the handle's choice (see
+ * spc5cuda_mat_set_kernel): through the length-sorted plan when the handle
+ * has one; the staged SpMM when every block-row fits the row kernels'
+ * buffers; the group SpMM for SPC5CUDA_KERNEL_GROUPS.  Up to 16 right-hand
+ * sides run in one pass over the matrix (fewer at larger r: at most 32
+ * accumulators per lane); larger k runs several passes. */
 SPC5CUDA_API spc5cuda_status spc5cuda_spmm(const spc5cuda_mat* mat, int k, const void* X,
                                            long ldx, void* Y, long ldy, void* stream);
 SPC5CUDA_API spc5cuda_status spc5cuda_spmm_mixed(const spc5cuda_mat* mat, int k, const float* X,
