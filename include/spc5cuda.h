@@ -178,12 +178,11 @@ SPC5CUDA_API spc5cuda_status spc5cuda_mat_info(const spc5cuda_mat* mat, spc5cuda
 
 /* SpMV kernel selection (no counterpart in the reference, which has one
  * kernel per r and instruction set).  Both kernels give the same bits.
- *   AUTO   -- for r <= 4, the thread-per-sub-row kernel when every
- *             block-row fits its per-warp staging buffers (stencils, Poisson,
- *             banded); the length-sorted plan (below) when some block-row
- *             does not; otherwise the group kernel (one group of VS lanes
- *             per block-row stream);
- *   GROUPS -- always the group kernel;
+ *   AUTO   -- the thread-per-sub-row kernel when every block-row fits its
+ *             per-warp staging buffers (stencils, Poisson, banded); the
+ *             length-sorted plan (below) when some block-row does not;
+ *   GROUPS -- always the group kernel (one group of VS lanes per block-row
+ *             stream);
  *   ROWS   -- the thread-per-sub-row kernel; SPC5CUDA_ERR_UNSUPPORTED on a
  *             converted matrix with a block-row that does not fit;
  *   SORTED -- the length-sorted plan: the handle keeps a second copy of the

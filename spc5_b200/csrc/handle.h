@@ -225,13 +225,11 @@ struct spc5cuda_mat {
         return v;
     }
     // The thread-per-sub-row kernel runs when every block-row fits its
-    // staging buffers: on request, or by default for r <= 4 (at r = 8 every
-    // block costs eight lanes a header decode each, and the group kernel is
-    // faster on the B200).
+    // staging buffers, on request or by default (it is faster than the group
+    // kernel on the B200 for every r).
     bool use_rows() const {
         if (!rows_ok || nwarps <= 0) return false;
-        if (kernel == SPC5CUDA_KERNEL_ROWS) return true;
-        return kernel == SPC5CUDA_KERNEL_AUTO && r <= 4;
+        return kernel == SPC5CUDA_KERNEL_ROWS || kernel == SPC5CUDA_KERNEL_AUTO;
     }
     // The length-sorted plan runs on request, or by default when some
     // block-row is too large for the row kernel (irregular matrices).

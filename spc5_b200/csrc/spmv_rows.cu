@@ -42,6 +42,68 @@ constexpr int ROWS_CTAS_PER_SM = 16;
 template <class LT, int R, class V, int L>
 using RowGeo = rows::Geo<LT, R, V, L>;
 
+// The blocks [b, b_stop) of a staged chunk for the lane that owns sub-row q
+// of its block-row and all VS columns (acc[c / CPL][c % CPL] is column c).
+// Its values in a block are contiguous: after those of the sub-rows below q,
+// one per set bit of its mask, in column order.
+template <class LT, int R, class V, class X, class A, int CPL>
+__device__ __forceinline__ void rows_subrow_blocks(const uint32_t* hw, long h_al, const V* vbuf,
+                                                   const X* __restrict__ x, int q, int& b, int b_stop, int& v,
+                                                   uint64_t pol_x, A (&acc)[R][CPL]) {
+    constexpr int VS = Layout<LT>::VS, MB = Layout<LT>::MASK_BYTES;
+    constexpr int MW = Header<LT, R>::MASK_WORDS, STRIDE = Header<LT, R>::STRIDE;
+    constexpr int FPW = 4 / MB, BITS = 8 * MB;
+    constexpr uint32_t FMASK = MB == 1 ? 0xFFu : 0xFFFFu;
+    constexpr int UT = 16 / VS > 1 ? 16 / VS : 1;  // blocks per step
+    const int wq = q / FPW;
+    const unsigned sh = unsigned(q % FPW) * BITS;
+    uint32_t lowmask[MW];  // mask bits of the sub-rows below q
+#pragma unroll
+    for (int w = 0; w < MW; ++w) lowmask[w] = w < wq ? 0xFFFFFFFFu : (w == wq ? (1u << sh) - 1u : 0u);
+    while (__any_sync(FULL, b < b_stop)) {
+        int col[UT];
+        uint32_t mw[UT][MW];
+        uint32_t mi[UT];
+#pragma unroll
+        for (int u = 0; u < UT; ++u) {
+            col[u] = 0;
+#pragma unroll
+            for (int w = 0; w < MW; ++w) mw[u][w] = 0u;
+            if (b + u < b_stop) col[u] = rows::decode_staged<LT, R>(hw, long(b + u) * STRIDE - h_al, mw[u]);
+            uint32_t word = mw[u][0];
+#pragma unroll
+            for (int w = 1; w < MW; ++w) word = w == wq ? mw[u][w] : word;
+            mi[u] = (word >> sh) & FMASK;
+        }
+        X xk[UT][VS];
+#pragma unroll
+        for (int u = 0; u < UT; ++u) {
+            const X* xp = x + col[u];
+#pragma unroll
+            for (int c = 0; c < VS; ++c) xk[u][c] = ((mi[u] >> c) & 1u) ? ld_x(xp + c, pol_x) : X(0);
+        }
+#pragma unroll
+        for (int u = 0; u < UT; ++u) {
+            int pre = 0, tot = 0;
+#pragma unroll
+            for (int w = 0; w < MW; ++w) {
+                pre += __popc(mw[u][w] & lowmask[w]);
+                tot += __popc(mw[u][w]);
+            }
+            int idx = v + pre;
+#pragma unroll
+            for (int c = 0; c < VS; ++c) {
+                if ((mi[u] >> c) & 1u) {
+                    acc[c / CPL][c % CPL] = fma(A(vbuf[idx]), A(xk[u][c]), acc[c / CPL][c % CPL]);
+                    ++idx;
+                }
+            }
+            v += tot;
+        }
+        b += UT;
+    }
+}
+
 // SEG: the block-rows are segments of long block-rows (the length-sorted
 // plan's largest ones), laid out so that chunk k of warp w holds segment k of
 // each of the block-rows w * 32 / L + slot (nseg of them, ng = min(32 / L,
@@ -62,6 +124,12 @@ __global__ void __launch_bounds__(ROWS_THREADS)
     constexpr uint32_t FMASK = MB == 1 ? 0xFFu : 0xFFFFu;
     constexpr bool Y_ATOMIC = sizeof(Y) == 8;  // red.add.f64 is y + s rounded once
     constexpr int CPL = VS / L;  // columns per lane
+    // r = 8 (L = 8): lane q owns sub-row q for all VS columns instead (the
+    // same R * CPL = VS accumulators, held per column: acc[c / CPL][c % CPL]).
+    // A power-law block holds about 2 of its 64 values, and a column lane
+    // would pay the offset arithmetic of 8 mask fields per block; a sub-row
+    // lane finds its values contiguous, after the masks below its own.
+    constexpr bool TRANS = R == 8 && L == 8;
     extern __shared__ __align__(16) unsigned char smem[];
 
     const int lane = threadIdx.x & 31;
@@ -90,6 +158,16 @@ __global__ void __launch_bounds__(ROWS_THREADS)
     // y[brow * R + q] += sum of sub-row q (warp-uniform call).
     auto flush = [&](bool mine, int brow) {
         A res = A(0);
+        if constexpr (TRANS) {
+            // the whole tree inside the lane: column c in acc[c / CPL][c % CPL]
+#pragma unroll
+            for (int d = VS / 2; d >= 1; d >>= 1) {
+#pragma unroll
+                for (int c = 0; c < d; ++c)
+                    acc[c / CPL][c % CPL] = acc[c / CPL][c % CPL] + acc[(c + d) / CPL][(c + d) % CPL];
+            }
+            res = acc[0][0];
+        } else {
 #pragma unroll
         for (int i = 0; i < R; ++i) {
 #pragma unroll
@@ -101,6 +179,7 @@ __global__ void __launch_bounds__(ROWS_THREADS)
 #pragma unroll
             for (int d = L / 2; d >= 1; d >>= 1) sum = sum + __shfl_xor_sync(FULL, sum, d);
             if (i == q) res = sum;
+        }
         }
         if (mine && q < R) {
             const long yrow = long(brow) * R + q;
@@ -126,6 +205,9 @@ __global__ void __launch_bounds__(ROWS_THREADS)
         int v = (mine ? (slot > 0 ? v_prev : ch.v_lo) : 0) - ch.v_al;  // buffer index of the block's values
 
         if constexpr (!SEG) zero();
+        if constexpr (TRANS) {
+            rows_subrow_blocks<LT, R, V, X, A, CPL>(hw, ch.h_al, vbuf, x, q, b, b_stop, v, pol_x, acc);
+        } else {
         while (__any_sync(FULL, b < b_stop)) {
             int col[U];
             uint32_t mw[U][MW];
@@ -171,6 +253,7 @@ __global__ void __launch_bounds__(ROWS_THREADS)
                 v += tot;
             }
             b += U;
+        }
         }
         if constexpr (!SEG) flush(mine, mine ? (perm ? __ldg(perm + ch.r0 + slot) : ch.r0 + slot) : 0);
     };

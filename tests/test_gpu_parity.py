@@ -189,8 +189,8 @@ def test_both_kernels_bit_exact(cuda, tag, dt, r, kernel):
 
 
 def test_kernel_selection(cuda):
-    """AUTO picks the row kernel for a stencil and the group kernel for a
-    matrix with a block-row longer than the row kernel's buffers."""
+    """AUTO picks the row kernel for a stencil (every r) and the sorted plan
+    for a matrix with a block-row longer than the row kernel's buffers."""
     st = converted(M.stencil27(12), np.float64, 4)
     assert st.kernel == S.KERNEL_ROWS
     st.set_kernel(S.KERNEL_GROUPS)
@@ -198,9 +198,9 @@ def test_kernel_selection(cuda):
     st.set_kernel(S.KERNEL_AUTO)
     assert st.kernel == S.KERNEL_ROWS
     st8 = converted(M.stencil27(12), np.float64, 8)
-    assert st8.kernel == S.KERNEL_GROUPS  # AUTO keeps the group kernel at r = 8
-    st8.set_kernel(S.KERNEL_ROWS)
-    assert st8.kernel == S.KERNEL_ROWS
+    assert st8.kernel == S.KERNEL_ROWS  # r = 8: one lane per sub-row
+    st8.set_kernel(S.KERNEL_GROUPS)
+    assert st8.kernel == S.KERNEL_GROUPS
     d = converted(M.dense(4096), np.float64, 1)  # one block-row of 512 blocks: 2.5 KB of headers
     assert d.kernel == S.KERNEL_SORTED  # AUTO: a block-row does not fit the row kernel
     d.set_kernel(S.KERNEL_GROUPS)
