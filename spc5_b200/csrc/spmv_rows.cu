@@ -124,12 +124,13 @@ __global__ void __launch_bounds__(ROWS_THREADS)
     constexpr uint32_t FMASK = MB == 1 ? 0xFFu : 0xFFFFu;
     constexpr bool Y_ATOMIC = sizeof(Y) == 8;  // red.add.f64 is y + s rounded once
     constexpr int CPL = VS / L;  // columns per lane
-    // r = 8 (L = 8): lane q owns sub-row q for all VS columns instead (the
-    // same R * CPL = VS accumulators, held per column: acc[c / CPL][c % CPL]).
-    // A power-law block holds about 2 of its 64 values, and a column lane
-    // would pay the offset arithmetic of 8 mask fields per block; a sub-row
-    // lane finds its values contiguous, after the masks below its own.
-    constexpr bool TRANS = R == 8 && L == 8;
+    // L = r >= 2: lane q owns sub-row q for all VS columns instead (the same
+    // R * CPL = VS accumulators, held per column: acc[c / CPL][c % CPL]).  A
+    // column lane pays the offset arithmetic of every mask field per block; a
+    // sub-row lane finds its values contiguous, after the masks below its own.
+    // Not in the segmented part at r = 4, where the column lanes' x loads of 8
+    // blocks per step hide the gathers better (measured on B200).
+    constexpr bool TRANS = R >= 2 && L == R && !(R == 4 && SEG);
     extern __shared__ __align__(16) unsigned char smem[];
 
     const int lane = threadIdx.x & 31;
