@@ -20,8 +20,17 @@ namespace rows {
 
 constexpr int THREADS = 128;
 constexpr int WARPS = THREADS / 32;
-constexpr int HB = 2048;  // header bytes of one warp's staging buffer
-constexpr int VB = 8192;  // value bytes of one warp's staging buffer
+// One warp's staging buffer: 7.5 KB, so that 7 CTAs of 4 warps fit an SM
+// (measured on B200: 10 KB buffers, 5 per SM, were 3% slower on the
+// power-law matrix and 10% on the 27-point stencil; 5 KB chunks were too
+// small for the stencil).
+constexpr int HB = 1536;  // header bytes of one warp's staging buffer
+constexpr int VB = 6144;  // value bytes of one warp's staging buffer
+// The multi-RHS kernels are limited by registers to 4 CTAs per SM, so they
+// stage larger chunks (every block-row or segment cut for the buffers above
+// fits these).
+constexpr int MM_HB = 2048;
+constexpr int MM_VB = 8192;
 constexpr unsigned FULL = 0xffffffffu;
 
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
@@ -33,7 +42,7 @@ __device__ __forceinline__ void l2_prefetch(const void* p, uint32_t bytes) {
     if (bytes) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
 }
 
-template <class LT, int R, class V, int L>
+template <class LT, int R, class V, int L, int HB_ = HB, int VB_ = VB>
 struct Geo {
     static constexpr int VS = Layout<LT>::VS;
     static constexpr int MB = Layout<LT>::MASK_BYTES;
@@ -43,7 +52,7 @@ struct Geo {
     static_assert(L >= R && L <= Layout<LT>::VS && 32 % L == 0, "lanes per block-row");
     static constexpr int SPW = 32 / L;  // block-rows per chunk (L lanes each)
     static constexpr int EPU = 16 / int(sizeof(V));
-    static constexpr int BUF_BYTES = HB + VB;
+    static constexpr int BUF_BYTES = HB_ + VB_;
     static constexpr int SMEM = WARPS * BUF_BYTES;
 };
 
@@ -64,7 +73,7 @@ struct Chunk {
 // call compute(chunk, staged header words, staged values), repeat.  A chunk
 // holds at most `cap` (<= 32 / L) block-rows: as many as fit the buffer.  The
 // caller guarantees that every block-row alone fits the buffer.
-template <class LT, int R, class V, int L, class F>
+template <class LT, int R, class V, int L, int HB_ = HB, int VB_ = VB, class F>
 __device__ __forceinline__ void walk(const int* __restrict__ brptr, const uint8_t* __restrict__ headers,
                                      const V* __restrict__ values, const int* __restrict__ valptr,
                                      int r_begin, int r_stop, unsigned char* wbuf, F&& compute,
@@ -74,9 +83,9 @@ __device__ __forceinline__ void walk(const int* __restrict__ brptr, const uint8_
     if (r_begin >= r_stop) return;
     const int lane = threadIdx.x & 31;
     const uint32_t s_h = uint32_t(__cvta_generic_to_shared(wbuf));
-    const uint32_t s_v = s_h + uint32_t(HB);
+    const uint32_t s_v = s_h + uint32_t(HB_);
     const uint32_t* hw = reinterpret_cast<const uint32_t*>(wbuf);
-    const V* vbuf = reinterpret_cast<const V*>(wbuf + HB);
+    const V* vbuf = reinterpret_cast<const V*>(wbuf + HB_);
     const uint64_t pol_stream = l2_evict_first_policy();
     // end of this range's header bytes and values: prefetches stay inside
     const long h_stop = (long(__ldg(brptr + r_stop)) * S + 15) & ~15L;
@@ -111,7 +120,7 @@ __device__ __forceinline__ void walk(const int* __restrict__ brptr, const uint8_
         if (bd.cand) {
             const long hneed = ((long(ch.b_hi) * S + 15) & ~15L) - ch.h_al;
             const long vneed = long((ch.v_hi + EPU - 1) & ~(EPU - 1)) - ch.v_al;
-            fits = hneed <= HB && vneed * long(sizeof(V)) <= VB;
+            fits = hneed <= HB_ && vneed * long(sizeof(V)) <= VB_;
         }
         // the ends grow with the lane, so the fitting lanes are a prefix
         ch.nrow = __popc(__ballot_sync(FULL, fits));

@@ -56,7 +56,7 @@ __device__ __forceinline__ void mm_range(int nrows, const int* __restrict__ brpt
     constexpr int L = mm_lanes<LT, R, SEG>();  // lanes per block-row
     constexpr int CPL = VS / L;                // columns per lane: q + L k
     constexpr int LOGL = L == 16 ? 4 : (L == 8 ? 3 : (L == 4 ? 2 : (L == 2 ? 1 : 0)));
-    using G = rows::Geo<LT, R, V, L>;
+    using G = rows::Geo<LT, R, V, L, rows::MM_HB, rows::MM_VB>;
     constexpr int MB = G::MB, MW = G::MW;
     constexpr int FPW = 4 / MB;  // mask fields per 32-bit word
     constexpr int BITS = 8 * MB;
@@ -210,10 +210,12 @@ __device__ __forceinline__ void mm_range(int nrows, const int* __restrict__ brpt
     };
     if constexpr (SEG) {
         zero();
-        rows::walk<LT, R, V, L>(brptr, headers, values, valptr, r_begin, r_stop, wbuf, compute, ng);
+        rows::walk<LT, R, V, L, rows::MM_HB, rows::MM_VB>(brptr, headers, values, valptr, r_begin, r_stop, wbuf,
+                                                          compute, ng);
         flush(slot < ng, slot < ng ? __ldg(perm + seg_base + slot) : 0);
     } else {
-        rows::walk<LT, R, V, L>(brptr, headers, values, valptr, r_begin, r_stop, wbuf, compute);
+        rows::walk<LT, R, V, L, rows::MM_HB, rows::MM_VB>(brptr, headers, values, valptr, r_begin, r_stop, wbuf,
+                                                          compute);
     }
 }
 
@@ -226,7 +228,7 @@ __global__ void __launch_bounds__(rows::THREADS)
                 int nwarps, const int* __restrict__ perm, int nseg, const X* __restrict__ xm, long ldx, long xcs,
                 Y* __restrict__ ym, long ldy, long ycs) {
     constexpr int L = mm_lanes<LT, R, SEG>();
-    using G = rows::Geo<LT, R, V, L>;
+    using G = rows::Geo<LT, R, V, L, rows::MM_HB, rows::MM_VB>;
     extern __shared__ __align__(16) unsigned char smem[];
     const int wi = threadIdx.x >> 5;
     const int warp = blockIdx.x * rows::WARPS + wi;
@@ -243,7 +245,7 @@ __global__ void __launch_bounds__(rows::THREADS)
 template <class LT, int R, int KC, class V, class X, class A, class Y>
 __global__ void __launch_bounds__(rows::THREADS)
     k_spmm_rows_batch(const BatchMat* __restrict__ mats, const BatchJob* __restrict__ jobs, int njobs) {
-    using G = rows::Geo<LT, R, V, mm_lanes<LT, R, false>()>;
+    using G = rows::Geo<LT, R, V, mm_lanes<LT, R, false>(), rows::MM_HB, rows::MM_VB>;
     extern __shared__ __align__(16) unsigned char smem[];
     const int wi = threadIdx.x >> 5;
     const int nw = gridDim.x * rows::WARPS;
@@ -299,7 +301,7 @@ void spmm_rows_run(const BetaView& m, int k, const X* x, long ldx, long xcs, Y* 
         const int kc = spmm_rows_kc(Layout<LT>::VS, m.r, k - k0, SEG);
         dispatch_rkc<LT, SEG>(m.r, kc, [&](auto RC, auto KCC) {
             constexpr int R_ = decltype(RC)::value, KC_ = decltype(KCC)::value;
-            constexpr int SMEM = rows::Geo<LT, R_, V, mm_lanes<LT, R_, SEG>()>::SMEM;
+            constexpr int SMEM = rows::Geo<LT, R_, V, mm_lanes<LT, R_, SEG>(), rows::MM_HB, rows::MM_VB>::SMEM;
             auto kern = k_spmm_rows<LT, R_, KC_, V, X, A, Y, SEG>;
             set_smem(kern, SMEM);
             kern<<<ctas, rows::THREADS, SMEM, s>>>(m.nrows, m.brptr, m.headers, vals, m.valptr, m.wstart,
@@ -328,7 +330,7 @@ void batch_rows_impl(int r, int kc, const BatchMat* mats, const BatchJob* jobs, 
                      cudaStream_t s) {
     dispatch_rkc<LT, false>(r, kc, [&](auto RC, auto KCC) {
         constexpr int R_ = decltype(RC)::value, KC_ = decltype(KCC)::value;
-        constexpr int SMEM = rows::Geo<LT, R_, V, mm_lanes<LT, R_, false>()>::SMEM;
+        constexpr int SMEM = rows::Geo<LT, R_, V, mm_lanes<LT, R_, false>(), rows::MM_HB, rows::MM_VB>::SMEM;
         auto kern = k_spmm_rows_batch<LT, R_, KC_, V, X, A, Y>;
         set_smem(kern, SMEM);
         int per_sm = 0;
