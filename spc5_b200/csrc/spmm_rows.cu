@@ -2,17 +2,20 @@
 // block-row fits the row kernels' staging buffers (rows_stage.cuh).
 //
 // A warp walks its block-rows in chunks staged into shared memory; each
-// block-row of a chunk is served by VS lanes, and lane c owns column c of
-// every block for all R sub-rows and KC right-hand sides (R * KC
-// accumulators).  Per block a lane decodes the staged header once, loads its
-// KC x values (only where some sub-row has a value in column c: blocks at the
-// right edge may reach past the last column), reads each of its sub-row
-// values once from shared memory and issues KC multiply-adds with it.
+// block-row of a chunk is served by L lanes (mm_lanes), and lane q owns the
+// columns q + L k of every block for all R sub-rows and KC right-hand sides
+// (R * VS / L * KC accumulators, at most 32).  Per block a lane decodes the
+// staged header once, loads its KC x values per column (only where some
+// sub-row has a value in that column: blocks at the right edge may reach
+// past the last column), reads each of its values once from shared memory
+// and issues KC multiply-adds with it.  The sorted plan's parts run here too
+// (the block-row permutation, and the segments of its largest block-rows).
 //
 // Arithmetic per right-hand side j is the SpMV's (src/spc5.hpp:2309-2715):
 // accumulator (i, j) of column c receives fma(value, x[col + c][j], acc) for
 // every block in order whose mask i has bit c; the row sum is the
-// _mm512_reduce_add tree over the VS lanes (XOR distances VS/2, ..., 1); then
+// _mm512_reduce_add tree over the VS columns (XOR distances VS/2, ..., 1: in
+// the lane, then across the L lanes); then
 // Y[row][j] += sum (one rounding: red.add.f64 for double Y, load-add-store for
 // float Y, exactly as the SpMV kernels).  Column j of the result is therefore
 // bit-identical to an SpMV with column j of X.

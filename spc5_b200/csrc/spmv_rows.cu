@@ -4,13 +4,16 @@
 // matrices).
 //
 // Work split: warp w owns the contiguous block-rows [wstart[w], wstart[w+1])
-// (balanced by blocks).  It walks them in chunks of at most 32 / r
-// block-rows: the chunk's packed headers and values are copied into the
-// warp's shared-memory buffers with coalesced 16-byte cp.async, then lane
-// (k*r + s) computes sub-row s of the k-th block-row of the chunk on its
-// own.  All VS column accumulators of that sub-row live in the lane's
-// registers, so a block costs one header decode and VS predicated
-// multiply-adds per sub-row -- no shuffles, no per-block broadcasts.
+// (balanced by blocks).  It walks them in chunks of at most 32 / L
+// block-rows (L lanes per block-row, L >= r): the chunk's packed headers and
+// values are copied into the warp's shared-memory buffer with coalesced
+// 16-byte cp.async (rows_stage.cuh), then the L lanes of each block-row work
+// on it from shared memory.  With L = r >= 2 lane s owns sub-row s and all VS
+// columns; otherwise lane q owns the columns q + L k of every sub-row.
+// Either way a lane holds r * VS / L accumulators in registers, a block
+// costs it one header decode and predicated multiply-adds, and the row sums
+// need at most log2(L) shuffles per block-row.  The sorted plan (plan.cu)
+// also runs this kernel on segments of block-rows too large to stage.
 //
 // Arithmetic (bit-identical to the reference kernels core_SPC5_{r}rVc_Spmv_*,
 // src/spc5.hpp:2309-2715): accumulator c of sub-row s receives
