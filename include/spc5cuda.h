@@ -200,6 +200,9 @@ SPC5CUDA_API spc5cuda_status spc5cuda_mat_info(const spc5cuda_mat* mat, spc5cuda
 #define SPC5CUDA_KERNEL_SORTED 3
 SPC5CUDA_API spc5cuda_status spc5cuda_mat_set_kernel(spc5cuda_mat* mat, int kernel);
 SPC5CUDA_API spc5cuda_status spc5cuda_mat_kernel(const spc5cuda_mat* mat, int* kernel);
+/* Kernel launches one spc5cuda_spmv of a converted handle makes now (one
+ * per part of the length-sorted plan, else 1; 0 for an empty matrix). */
+SPC5CUDA_API spc5cuda_status spc5cuda_mat_spmv_launches(const spc5cuda_mat* mat, int* launches);
 
 /* SPC5_{r}rVc_block_count (spc5.hpp:510-513, 635-638, 764-767, 890-893):
  * number of blocks the conversion to r would produce.  CSR handles only.

@@ -49,7 +49,7 @@ EXPORTED_SYMBOLS = [
     "spc5cuda_server_add_matrix", "spc5cuda_server_submit", "spc5cuda_server_wait",
     "spc5cuda_server_drain", "spc5cuda_server_get_stats", "spc5cuda_server_destroy",
     "spc5cuda_mat_create_coo", "spc5cuda_decode_coo", "spc5cuda_core_spmv_f64_noalloc",
-    "spc5cuda_mat_set_kernel", "spc5cuda_mat_kernel",
+    "spc5cuda_mat_set_kernel", "spc5cuda_mat_kernel", "spc5cuda_mat_spmv_launches",
 ]
 
 TUNE_MODEL = 0
@@ -131,6 +131,8 @@ def _lib():
         lib.spc5cuda_mat_set_kernel.argtypes = [_P, _I]
         lib.spc5cuda_mat_kernel.restype = _I
         lib.spc5cuda_mat_kernel.argtypes = [_P, C.POINTER(_I)]
+        lib.spc5cuda_mat_spmv_launches.restype = _I
+        lib.spc5cuda_mat_spmv_launches.argtypes = [_P, C.POINTER(_I)]
         lib.spc5cuda_block_count.restype = _I
         lib.spc5cuda_block_count.argtypes = [_P, _I, C.POINTER(_L), _P]
         lib.spc5cuda_convert.restype = _I
@@ -246,6 +248,14 @@ class SPC5Mat:
     def set_kernel(self, kernel: int) -> None:
         """Select the SpMV kernel: KERNEL_AUTO, KERNEL_GROUPS, KERNEL_ROWS or KERNEL_SORTED."""
         _check(_lib().spc5cuda_mat_set_kernel(self._h, int(kernel)), "spc5cuda_mat_set_kernel")
+
+    @property
+    def spmv_launches(self) -> int:
+        """Kernel launches one SPC5_Spmv of this converted matrix makes (one per part of the
+        length-sorted plan, else 1)."""
+        n = C.c_int(0)
+        _check(_lib().spc5cuda_mat_spmv_launches(self._h, C.byref(n)), "spc5cuda_mat_spmv_launches")
+        return n.value
 
     @property
     def kernel(self) -> int:

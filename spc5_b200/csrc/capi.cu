@@ -285,6 +285,16 @@ spc5cuda_status spc5cuda_mat_set_kernel(spc5cuda_mat* m, int kernel) {
     });
 }
 
+spc5cuda_status spc5cuda_mat_spmv_launches(const spc5cuda_mat* m, int* launches) {
+    return guarded([&] {
+        require(m && launches, SPC5CUDA_ERR_INVALID, "null");
+        require(m->r != 0, SPC5CUDA_ERR_FORMAT, "matrix is not converted");
+        if (m->nrows == 0) *launches = 0;
+        else if (m->use_plan()) *launches = int(m->plan->parts.size());
+        else *launches = 1;
+    });
+}
+
 spc5cuda_status spc5cuda_mat_kernel(const spc5cuda_mat* m, int* kernel) {
     return guarded([&] {
         require(m && kernel, SPC5CUDA_ERR_INVALID, "null");

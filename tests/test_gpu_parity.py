@@ -212,6 +212,7 @@ def test_kernel_selection(cuda):
         d.set_kernel(7)
     pl = converted(M.powerlaw(20000, seed=7), np.float64, 2)
     assert pl.kernel == S.KERNEL_SORTED
+    assert st.spmv_launches == 1 and pl.spmv_launches >= 2  # one launch per part of the plan
     before = pl.info().device_bytes
     pl.set_kernel(S.KERNEL_GROUPS)  # releases the sorted copy
     assert pl.kernel == S.KERNEL_GROUPS and pl.info().device_bytes < before
