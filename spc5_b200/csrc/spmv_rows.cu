@@ -176,17 +176,17 @@ __global__ void __launch_bounds__(ROWS_THREADS)
             res = acc[0][0];
         } else {
 #pragma unroll
-        for (int i = 0; i < R; ++i) {
+            for (int i = 0; i < R; ++i) {
 #pragma unroll
-            for (int d = CPL / 2; d >= 1; d >>= 1) {
+                for (int d = CPL / 2; d >= 1; d >>= 1) {
 #pragma unroll
-                for (int k = 0; k < d; ++k) acc[i][k] = acc[i][k] + acc[i][k + d];
+                    for (int k = 0; k < d; ++k) acc[i][k] = acc[i][k] + acc[i][k + d];
+                }
+                A sum = acc[i][0];
+#pragma unroll
+                for (int d = L / 2; d >= 1; d >>= 1) sum = sum + __shfl_xor_sync(FULL, sum, d);
+                if (i == q) res = sum;
             }
-            A sum = acc[i][0];
-#pragma unroll
-            for (int d = L / 2; d >= 1; d >>= 1) sum = sum + __shfl_xor_sync(FULL, sum, d);
-            if (i == q) res = sum;
-        }
         }
         if (mine && q < R) {
             const long yrow = long(brow) * R + q;
@@ -215,52 +215,52 @@ __global__ void __launch_bounds__(ROWS_THREADS)
         if constexpr (TRANS) {
             rows_subrow_blocks<LT, R, V, X, A, CPL>(hw, ch.h_al, vbuf, x, q, b, b_stop, v, pol_x, acc);
         } else {
-        while (__any_sync(FULL, b < b_stop)) {
-            int col[U];
-            uint32_t mw[U][MW];
+            while (__any_sync(FULL, b < b_stop)) {
+                int col[U];
+                uint32_t mw[U][MW];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                col[u] = 0;
+                for (int u = 0; u < U; ++u) {
+                    col[u] = 0;
 #pragma unroll
-                for (int w = 0; w < MW; ++w) mw[u][w] = 0u;
-                if (b + u < b_stop) col[u] = rows::decode_staged<LT, R>(hw, long(b + u) * G::STRIDE - ch.h_al, mw[u]);
-            }
-            // x of this lane's columns where some sub-row has a value
-            X xk[U][CPL];
+                    for (int w = 0; w < MW; ++w) mw[u][w] = 0u;
+                    if (b + u < b_stop) col[u] = rows::decode_staged<LT, R>(hw, long(b + u) * G::STRIDE - ch.h_al, mw[u]);
+                }
+                // x of this lane's columns where some sub-row has a value
+                X xk[U][CPL];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const uint32_t uni = rows::mask_union<LT, R>(mw[u]);
-                const X* xp = x + col[u] + q;
+                for (int u = 0; u < U; ++u) {
+                    const uint32_t uni = rows::mask_union<LT, R>(mw[u]);
+                    const X* xp = x + col[u] + q;
 #pragma unroll
-                for (int k = 0; k < CPL; ++k)
-                    xk[u][k] = ((uni >> (q + L * k)) & 1u) ? ld_x(xp + L * k, pol_x) : X(0);
-            }
+                    for (int k = 0; k < CPL; ++k)
+                        xk[u][k] = ((uni >> (q + L * k)) & 1u) ? ld_x(xp + L * k, pol_x) : X(0);
+                }
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                uint32_t pre[MW];
-                const int tot = rows::subrow_prefix<LT, R>(mw[u], pre);
+                for (int u = 0; u < U; ++u) {
+                    uint32_t pre[MW];
+                    const int tot = rows::subrow_prefix<LT, R>(mw[u], pre);
 #pragma unroll
-                for (int k = 0; k < CPL; ++k) {
-                    const int c = q + L * k;
-                    const uint32_t below = (1u << c) - 1u;
+                    for (int k = 0; k < CPL; ++k) {
+                        const int c = q + L * k;
+                        const uint32_t below = (1u << c) - 1u;
 #pragma unroll
-                    for (int w = 0; w < MW; ++w) {
-                        // field i: buffer offset of sub-row i's value in column c
-                        const uint32_t off = rows::column_offsets<LT, R>(mw[u][w], pre[w], below);
+                        for (int w = 0; w < MW; ++w) {
+                            // field i: buffer offset of sub-row i's value in column c
+                            const uint32_t off = rows::column_offsets<LT, R>(mw[u][w], pre[w], below);
 #pragma unroll
-                        for (int f = 0; f < FPW; ++f) {
-                            const int i = w * FPW + f;
-                            if (i < R && ((mw[u][w] >> (f * BITS + c)) & 1u)) {
-                                const int idx = v + int((off >> (f * BITS)) & FMASK);
-                                acc[i][k] = fma(A(vbuf[idx]), A(xk[u][k]), acc[i][k]);
+                            for (int f = 0; f < FPW; ++f) {
+                                const int i = w * FPW + f;
+                                if (i < R && ((mw[u][w] >> (f * BITS + c)) & 1u)) {
+                                    const int idx = v + int((off >> (f * BITS)) & FMASK);
+                                    acc[i][k] = fma(A(vbuf[idx]), A(xk[u][k]), acc[i][k]);
+                                }
                             }
                         }
                     }
+                    v += tot;
                 }
-                v += tot;
+                b += U;
             }
-            b += U;
-        }
         }
         if constexpr (!SEG) flush(mine, mine ? (perm ? __ldg(perm + ch.r0 + slot) : ch.r0 + slot) : 0);
     };
