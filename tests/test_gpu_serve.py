@@ -102,3 +102,28 @@ def test_shards_concatenate_to_full_spmv(cuda, r):
             parts.append(sh.spmv(x, y))
         torch.cuda.synchronize()
         assert torch.cat(parts).cpu().numpy().tobytes() == y_full.cpu().numpy().tobytes()
+
+
+def test_multi_server_places_routes_and_matches_solo(cuda):
+    """MultiServer over the GPUs of this run: the placement covers every
+    matrix, and each request's result equals a solo SpMV bit for bit on
+    whichever GPU the router picked."""
+    from spc5_b200 import serving as SV
+    n = torch.cuda.device_count()
+    csrs = [M.powerlaw(20000, seed=3), M.stencil27(18), M.banded(7000, 40, 0.2, seed=5)]
+    rs = (1, 4, 2)
+    ms = SV.MultiServer(n_gpus=n, slots=2, max_k=8)
+    ids = ms.add_matrices(csrs, [0.6, 0.3, 0.1], [S.FORMAT_OF_R[r] for r in rs])
+    assert all(len(gs) >= 1 for gs in ms.placement)
+    mats = [converted(c, np.float64, r) for c, r in zip(csrs, rs)]
+    pending = []
+    for q in range(24):
+        i = q % 3
+        x = torch.from_numpy(M.x_vector(csrs[i].ncols, 50 + q, np.float64)).cuda()
+        y = torch.empty(csrs[i].nrows, dtype=torch.float64, device="cuda")
+        pending.append((i, x, y, ms.submit(ids[i], x, y)))
+    for i, x, y, rid in pending:
+        assert ms.wait(rid) >= 0.0
+        assert y.cpu().numpy().tobytes() == solo(mats[i], x, False).cpu().numpy().tobytes()
+    assert all(v == 0 for v in ms.router.outstanding)
+    ms.close()
