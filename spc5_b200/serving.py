@@ -115,26 +115,28 @@ class MultiServer:
     server.  ``submit(mat, x, y)`` copies x to the chosen GPU, queues
     ``y = A x`` there and returns a request id; ``wait(rid)`` copies the result
     into y (any device) and returns the latency in microseconds seen by that
-    GPU's request loop.
+    GPU's request loop.  A wait that raises (a timeout, a device error) keeps
+    the request outstanding, so the caller can wait on it again.
+
+    The device work goes through the methods ``_device_count``, ``_device``,
+    ``_free_bytes``, ``_new_server``, ``_convert``, ``_stage`` and
+    ``_copy_out``, so that the placement, routing and bookkeeping can be
+    exercised without GPUs.
     """
 
     def __init__(self, n_gpus=None, slots=4, max_k=16, mixed=False, hbm_fraction=0.9):
         self.slots, self.max_k = int(slots), int(max_k)
-        import torch
-
-        from . import Server
-        self.n = torch.cuda.device_count() if n_gpus is None else int(n_gpus)
+        self.n = self._device_count() if n_gpus is None else int(n_gpus)
         if self.n < 1:
             raise RuntimeError("MultiServer needs a CUDA device")
         self.mixed = bool(mixed)
         self.capacity = []
         self.servers = []
         for g in range(self.n):
-            with torch.cuda.device(g):
-                free, _ = torch.cuda.mem_get_info()
+            with self._device(g):
+                free = self._free_bytes()
                 self.capacity.append(int(free * hbm_fraction))
-                self.servers.append(Server(slots=slots, max_k=max_k, mixed=mixed,
-                                           hbm_budget=int(free * hbm_fraction)))
+                self.servers.append(self._new_server(int(free * hbm_fraction)))
         self.placement = []
         self.ids = []      # per matrix: {gpu: id on that gpu's server}
         self.handles = []  # keeps the per-GPU handles alive
@@ -142,19 +144,54 @@ class MultiServer:
         self._reqs = {}
         self._next = 1
 
+    # ---- device hooks ---------------------------------------------------
+    def _device_count(self) -> int:
+        import torch
+        return torch.cuda.device_count()
+
+    def _device(self, g):
+        import torch
+        return torch.cuda.device(g)
+
+    def _free_bytes(self) -> int:
+        import torch
+        free, _ = torch.cuda.mem_get_info()
+        return int(free)
+
+    def _new_server(self, budget: int):
+        from . import Server
+        return Server(slots=self.slots, max_k=self.max_k, mixed=self.mixed, hbm_budget=budget)
+
+    def _convert(self, csr, fmt):
+        """A converted handle of ``csr`` on the current device."""
+        from . import CSR_to_SPC5, csr_matrix
+        dt = np.float32 if self.mixed else np.float64
+        m = csr_matrix(csr.rowptr, csr.colidx, csr.values.astype(dt), csr.ncols)
+        CSR_to_SPC5(m, fmt)
+        return m
+
+    def _stage(self, g, x, nrows):
+        """x on GPU g and a result vector there; the request loop's stream
+        must see the copy of x."""
+        import torch
+        dev = torch.device("cuda", g)
+        xg = x.to(dev, non_blocking=True)
+        yg = torch.empty(nrows, dtype=torch.float64, device=dev)
+        torch.cuda.current_stream(dev).synchronize()
+        return xg, yg
+
+    def _copy_out(self, y, yg) -> None:
+        y.copy_(yg)
+
+    # ---- requests ---------------------------------------------------------
     def add_matrices(self, csrs, shares, formats):
         """Places and registers ``csrs`` (``matrices.CSR``); ``formats[i]`` is
         the beta(r,VS) format of matrix i (``FORMAT_OF_R[r]``)."""
-        import torch
-
-        from . import CSR_to_SPC5, csr_matrix
-        dt = np.float32 if self.mixed else np.float64
         # footprint of one replica: measured on the first GPU that converts it
         footprints = []
         for csr, fmt in zip(csrs, formats):
-            with torch.cuda.device(0):
-                m = csr_matrix(csr.rowptr, csr.colidx, csr.values.astype(dt), csr.ncols)
-                CSR_to_SPC5(m, fmt)
+            with self._device(0):
+                m = self._convert(csr, fmt)
                 footprints.append(int(m.info().device_bytes))
                 del m
         # every server also keeps its slots' staging blocks (max_k columns of
@@ -168,37 +205,44 @@ class MultiServer:
         for i, (csr, fmt) in enumerate(zip(csrs, formats)):
             ids = {}
             for g in placement[i]:
-                with torch.cuda.device(g):
-                    m = csr_matrix(csr.rowptr, csr.colidx, csr.values.astype(dt), csr.ncols)
-                    CSR_to_SPC5(m, fmt)
+                with self._device(g):
+                    m = self._convert(csr, fmt)
                     ids[g] = self.servers[g].add_matrix(m)
                     self.handles.append(m)
             self.placement.append(placement[i])
             self.ids.append(ids)
-        self.router = Router(self.placement, self.n)
+        if self.router is None:
+            self.router = Router(self.placement, self.n)
+        else:
+            # keep the outstanding counts of requests already submitted
+            self.router.placement = [list(gs) for gs in self.placement]
         return list(range(base, base + len(csrs)))
 
     def submit(self, mat: int, x, y) -> int:
-        import torch
         g = self.router.pick(mat)
-        dev = torch.device("cuda", g)
-        with torch.cuda.device(g):
-            xg = x.to(dev, non_blocking=True)
-            yg = torch.empty(y.shape[0], dtype=torch.float64, device=dev)
-            # the request loop's stream must see the copy of x
-            torch.cuda.current_stream(dev).synchronize()
-            rid = self.servers[g].submit(self.ids[mat][g], xg, yg)
+        try:
+            with self._device(g):
+                xg, yg = self._stage(g, x, y.shape[0])
+                rid = self.servers[g].submit(self.ids[mat][g], xg, yg)
+        except BaseException:
+            self.router.done(g)
+            raise
         key = self._next
         self._next += 1
         self._reqs[key] = (g, rid, xg, yg, y)
         return key
 
     def wait(self, key: int, timeout_s: float = 60.0) -> float:
-        g, rid, _, yg, y = self._reqs.pop(key)
-        lat = self.servers[g].wait(rid, timeout_s)
-        y.copy_(yg)
+        g, rid, _, yg, y = self._reqs[key]
+        lat = self.servers[g].wait(rid, timeout_s)  # raises: still outstanding
+        self._copy_out(y, yg)
+        del self._reqs[key]
         self.router.done(g)
         return lat
+
+    def outstanding(self) -> list:
+        """Requests submitted and not yet waited for, per GPU."""
+        return list(self.router.outstanding) if self.router else [0] * self.n
 
     def gpu_of(self, key: int) -> int:
         return self._reqs[key][0]
