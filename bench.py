@@ -15,9 +15,11 @@ y += A x per format (4 SpMV launches), inputs resident in HBM.
   copied back, every step.
 * ``roofline``-- the SpMV kernel: algorithmic bytes per launch / mean
   CUDA-event launch time, against the measured HBM copy bandwidth.
-* ``mixed``   -- the same matrix in the f32 beta(r,16) layout with FP32 x
-  and FP64 accumulation: GB/s, SpMV/s ratio to FP64 and max relative error
-  against the FP64 path (which is bit-identical to the reference).
+* ``mixed``   -- the same matrix with float values in the 8-column layout
+  (uint8 masks), FP32 x and FP64 accumulation: GB/s, SpMV/s ratio to FP64
+  and the error against an FP64 CSR product (per row relative to
+  sum_j |a_ij x_j|, and normwise); ``mixed.f32_layout`` is the same for the
+  reference's float layout beta(r,16).
 * ``cpu_baseline`` -- the reference's own AVX-512 OpenMP SpMV
   (SPC5_Spmv_omp, src/spc5.hpp compiled by oracle/Makefile) on this host.
 
@@ -285,6 +287,68 @@ def run_reference(args):
 # GPU path
 # ---------------------------------------------------------------------------
 
+def fp64_csr_reference(csr, x):
+    """FP64 CSR product y = A x and sum_j |a_ij x_j| per row, on the device
+    (cuSPARSE through torch.sparse): the yardstick of the mixed-precision
+    error, independent of the beta kernels."""
+    import torch
+    rp = torch.from_numpy(csr.rowptr.astype(np.int64)).cuda()
+    ci = torch.from_numpy(csr.colidx.astype(np.int64)).cuda()
+    va = torch.from_numpy(csr.values).cuda()
+    a = torch.sparse_csr_tensor(rp, ci, va, (csr.nrows, csr.ncols))
+    y = (a @ x.unsqueeze(1)).squeeze(1)
+    a_abs = torch.sparse_csr_tensor(rp, ci, va.abs(), (csr.nrows, csr.ncols))
+    absrow = (a_abs @ x.abs().unsqueeze(1)).squeeze(1)
+    del a, a_abs, rp, ci, va
+    return y, absrow
+
+
+def mixed_legs(csr, mats, x, per_r_ms, args, stream, select_kernel):
+    """Mixed precision on the bench matrix for every format: GB/s, SpMV/s
+    relative to the FP64 path, and the error against an FP64 CSR product.
+    ``mixed`` is the 8-column layout (F32_V8: float values, uint8 masks);
+    ``f32_layout`` the reference's float layout beta(r,16)."""
+    import torch
+    import spc5_b200 as S
+    y64, absrow = fp64_csr_reference(csr, x)
+    x32 = x.float()
+    out = {}
+    for name, vt, (sv, mb) in (("v8", S.F32_V8, (4, 1)), ("f32_layout", S.F32, (4, 2))):
+        ms_total, fp64_total, nbytes, comp, normw = 0.0, 0.0, 0, 0.0, 0.0
+        for r, _m64 in mats:
+            mm = S.csr_matrix(csr.rowptr, csr.colidx, csr.values, csr.ncols, dtype=np.float32, value_type=vt)
+            S.CSR_to_SPC5(mm, S.FORMAT_OF_R[r])
+            select_kernel(mm, args.kernel)
+            ym = torch.zeros(csr.nrows, dtype=torch.float64, device="cuda")
+            S.SPC5_Spmv_mixed(mm, x32, ym)
+            torch.cuda.synchronize()
+            d = (ym - y64).abs()
+            comp = max(comp, (d / absrow.clamp_min(1e-300)).max().item())
+            normw = max(normw, (d.max() / y64.abs().max()).item())
+            for _ in range(args.warmup):
+                S.SPC5_Spmv_mixed(mm, x32, ym)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(args.steps):
+                S.SPC5_Spmv_mixed(mm, x32, ym)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms_total += a.elapsed_time(b) / args.steps
+            fp64_total += per_r_ms[r]
+            nbytes += spmv_bytes(csr.nnz, mm.numberOfBlocks, r, csr.nrows, csr.ncols, sv, mb, 4, 8)
+            del mm, ym
+        out[name] = {"gbs": round(nbytes / (ms_total * 1e-3) / 1e9, 2),
+                     "spmv_per_s_ratio_vs_fp64": round(fp64_total / ms_total, 3),
+                     "max_componentwise_rel_err_vs_fp64_csr": comp,
+                     "normwise_rel_err_vs_fp64_csr": normw}
+    del y64, absrow
+    res = dict(out["v8"])
+    res["layout"] = "float values in the 8-column layout (uint8 masks), FP32 x, FP64 accumulation and y"
+    res["error_reference"] = "FP64 CSR product of the unrounded matrix and x (cuSPARSE via torch); componentwise = max_i |dy_i| / sum_j |a_ij x_j|"
+    res["f32_layout"] = out["f32_layout"]
+    return res
+
+
 def run_gpu(args):
     import torch
     import torch.distributed as dist
@@ -420,38 +484,14 @@ def run_gpu(args):
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
     e2e_value = step_bytes * args.steps * world / (e2e_ms * 1e-3) / 1e9
 
-    # ---- mixed precision on the same matrix (f32 beta(r,16), FP64 y) ----
+    # ---- mixed precision on the same matrix: float values and x, FP64
+    # accumulation and y, in the 8-column layout (F32_V8, the default) and in
+    # the reference's float layout (beta(r,16)); the error is stated against an
+    # FP64 CSR product of the unrounded matrix and x on the device (cuSPARSE
+    # through torch), per row relative to sum_j |a_ij x_j| and normwise
     mixed = {}
     if not args.no_mixed:
-        y_ref = torch.zeros_like(y)
-        x32 = x.float()
-        mixed_ms_total, fp64_ms_total, mixed_bytes, max_rel = 0.0, 0.0, 0, 0.0
-        for r, m64 in mats:
-            m32 = S.csr_matrix(csr.rowptr, csr.colidx, csr.values, csr.ncols, dtype=np.float32)
-            S.CSR_to_SPC5(m32, S.FORMAT_OF_R[r])
-            select_kernel(m32, args.kernel)
-            ym = torch.zeros_like(y)
-            y_ref.zero_()
-            S.SPC5_Spmv(m64, x, y_ref)
-            S.SPC5_Spmv_mixed(m32, x32, ym)
-            torch.cuda.synchronize()
-            rel = ((ym - y_ref).abs().max() / y_ref.abs().max()).item()
-            max_rel = max(max_rel, rel)
-            for _ in range(args.warmup):
-                S.SPC5_Spmv_mixed(m32, x32, ym)
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            for _ in range(args.steps):
-                S.SPC5_Spmv_mixed(m32, x32, ym)
-            b.record(stream)
-            torch.cuda.synchronize()
-            mixed_ms_total += a.elapsed_time(b) / args.steps
-            fp64_ms_total += per_r_ms[r]
-            mixed_bytes += spmv_bytes(csr.nnz, m32.numberOfBlocks, r, csr.nrows, csr.ncols, 4, 2, 4, 8)
-            del m32
-        mixed = {"gbs": round(mixed_bytes / (mixed_ms_total * 1e-3) / 1e9, 2),
-                 "spmv_per_s_ratio_vs_fp64": round(fp64_ms_total / mixed_ms_total, 3),
-                 "normwise_rel_err_vs_fp64": max_rel, "layout": "f32 beta(r,16), FP32 x, FP64 y"}
+        mixed = mixed_legs(csr, mats, x, per_r_ms, args, stream, select_kernel)
 
     traffic, traffic_src = args.traffic, "ncu (given)" if args.traffic else None
     ratios = TRAFFIC_RATIO.get(args.workload)
@@ -535,7 +575,8 @@ def run_batched(args):
         tdt = torch.float32 if mixed else torch.float64
         mats, Xs, Ys, total_bytes, flops, chosen = [], [], [], 0, 0, {}
         for csr, k in work:
-            m = S.csr_matrix(csr.rowptr, csr.colidx, csr.values.astype(dt), csr.ncols)
+            m = S.csr_matrix(csr.rowptr, csr.colidx, csr.values.astype(dt), csr.ncols,
+                             value_type=S.F32_V8 if mixed else None)
             r = S.autotune(m, S.TUNE_MODEL)["r"]
             S.CSR_to_SPC5(m, S.FORMAT_OF_R[r])
             chosen[r] = chosen.get(r, 0) + 1
@@ -543,7 +584,7 @@ def run_batched(args):
             Xs.append(torch.from_numpy(np.random.default_rng(len(Xs)).uniform(-1, 1, (csr.ncols, k))).to(
                 "cuda", tdt))
             Ys.append(torch.zeros(csr.nrows, k, dtype=torch.float64 if mixed else tdt, device="cuda"))
-            sv, mb, sx = (4, 2, 4) if mixed else (8, 1, 8)
+            sv, mb, sx = (4, 1, 4) if mixed else (8, 1, 8)
             nbr = (csr.nrows + r - 1) // r
             total_bytes += (csr.nnz * sv + m.numberOfBlocks * (4 + r * mb) + 4 * (nbr + 1) +
                             k * (csr.ncols * sx + 2 * csr.nrows * 8))
@@ -611,7 +652,8 @@ def run_serve(args):
         mats = []
         for rep in range(8):
             for csr in distinct:
-                m = S.csr_matrix(csr.rowptr, csr.colidx, csr.values.astype(dt), csr.ncols)
+                m = S.csr_matrix(csr.rowptr, csr.colidx, csr.values.astype(dt), csr.ncols,
+                                 value_type=S.F32_V8 if mixed else None)
                 # default kernel choice: lone requests run the handle's SpMV
                 # (the length-sorted copy for the power-law matrices), batches
                 # the SpMM on the handle's own arrays

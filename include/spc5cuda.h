@@ -48,8 +48,12 @@ enum spc5cuda_format {
     SPC5CUDA_FORMAT_8rVc = 5
 };
 
-/* Value types of a matrix: SPC5Mat<double> (VS = 8) or SPC5Mat<float> (VS = 16). */
-enum spc5cuda_value_type { SPC5CUDA_F64 = 0, SPC5CUDA_F32 = 1 };
+/* Value types of a matrix: SPC5Mat<double> (VS = 8) or SPC5Mat<float> (VS = 16).
+ * SPC5CUDA_F32_V8 (no counterpart in the reference) stores float values in
+ * the 8-column layout of SPC5Mat<double> (uint8 masks, headers identical to
+ * the double conversion of the same pattern); it serves the mixed-precision
+ * calls (float x, FP64 accumulation and y) with half the value bytes of F64. */
+enum spc5cuda_value_type { SPC5CUDA_F64 = 0, SPC5CUDA_F32 = 1, SPC5CUDA_F32_V8 = 2 };
 
 /* Status codes (the reference throws std::invalid_argument for an unknown
  * format, spc5.hpp:1014; errors never cross this ABI as exceptions). */
@@ -224,8 +228,13 @@ SPC5CUDA_API spc5cuda_status spc5cuda_get_arrays(const spc5cuda_mat* mat, int* r
  * of the handle's value type. */
 SPC5CUDA_API spc5cuda_status spc5cuda_spmv(const spc5cuda_mat* mat, const void* x, void* y, void* stream);
 
-/* Mixed precision (no counterpart in the reference): an F32 handle, float
- * x, double y; FP64 per-lane accumulation and FP64 row reduction. */
+/* Mixed precision (no counterpart in the reference): an F32 or F32_V8
+ * handle, float x, double y; FP64 per-lane accumulation and FP64 row
+ * reduction.  On an F32_V8 handle each chain is the FP64 kernel's chain on
+ * the float values and float x widened to double (their product is exact in
+ * FP64), so y equals spc5cuda_spmv on the F64 matrix of the rounded values
+ * and x.  spc5cuda_spmv and spc5cuda_spmm reject F32_V8 handles
+ * (SPC5CUDA_ERR_FORMAT): only the mixed calls take them. */
 SPC5CUDA_API spc5cuda_status spc5cuda_spmv_mixed(const spc5cuda_mat* mat, const float* x, double* y,
                                     void* stream);
 

@@ -155,6 +155,23 @@ def beta_spmv_mixed(r, nrows, brptr, headers, values, x, y):
     return y
 
 
+def beta_spmv_mixed8(r, nrows, brptr, headers, values, x, y):
+    """Mixed precision in the 8-column layout (float values with the headers
+    of the double conversion, float x, FP64 y): every chain is the FP64
+    kernel's chain on the values and x widened to double -- the product of two
+    floats is exact in FP64 -- so this is beta_spmv_f64 on the widened arrays
+    (core_SPC5_{r}rVc_Spmv_double, src/spc5.hpp:2309-2632)."""
+    return beta_spmv_f64(r, nrows, brptr, headers, np.asarray(values, dtype=np.float32).astype(np.float64),
+                         np.asarray(x, dtype=np.float32).astype(np.float64), y)
+
+
+def csr_to_beta_v8(r, rowptr, colidx, values):
+    """Arrays of the 8-column layout with float values: the double conversion
+    of the pattern (src/spc5.hpp:165-228), values rounded to float."""
+    b, h, v = csr_to_beta(r, rowptr, colidx, np.asarray(values, dtype=np.float32).astype(np.float64))
+    return b, h, v.astype(np.float32)
+
+
 def csr_spmv_f64(rowptr, colidx, values, x, y):
     """y += A x row by row (CSR_Spmv_scalar); returns (y, sum_j |a_ij x_j| per row)."""
     rowptr, colidx = _i32(rowptr), _i32(colidx)

@@ -34,6 +34,8 @@ SPC5_VEC_PADDING_Y = 7
 
 F64 = 0
 F32 = 1
+# float values in the 8-column layout of SPC5Mat<double> (mixed-precision calls only)
+F32_V8 = 2
 
 EXPORTED_SYMBOLS = [
     "spc5cuda_status_string", "spc5cuda_get_last_error", "spc5cuda_set_stream",
@@ -291,7 +293,12 @@ class SPC5Mat:
 
     @property
     def dtype(self):
+        """Value dtype (float32 for both F32 and F32_V8 handles)."""
         return np.float64 if self.info().value_type == F64 else np.float32
+
+    @property
+    def value_type(self) -> int:
+        return self.info().value_type
 
     def arrays(self):
         """Host copies of (rowsSize, blocksColumnIndexesWithMasks, values)."""
@@ -307,12 +314,15 @@ class SPC5Mat:
         return brptr, headers, values
 
 
-def csr_matrix(rowptr, colidx, values, ncols: int, dtype=None, stream=None) -> SPC5Mat:
+def csr_matrix(rowptr, colidx, values, ncols: int, dtype=None, stream=None, value_type=None) -> SPC5Mat:
     """A CSR ``SPC5Mat`` from host numpy arrays or CUDA tensors (int32
     indices, sorted columns per row).  ``dtype`` (float64/float32) casts the
     values; float32 gives the VS = 16 layout used by the float and mixed
-    kernels."""
+    kernels.  ``value_type=F32_V8`` casts the values to float32 and keeps the
+    8-column layout of the double format (the mixed-precision calls only)."""
     import torch
+    if value_type == F32_V8:
+        dtype = np.float32
     on_device = isinstance(rowptr, torch.Tensor) and rowptr.is_cuda
     if on_device:
         vals = values if dtype is None else values.to(getattr(torch, np.dtype(dtype).name))
@@ -331,6 +341,8 @@ def csr_matrix(rowptr, colidx, values, ncols: int, dtype=None, stream=None) -> S
         nnz = len(ci)
         ptrs = (_np_ptr(rp), _np_ptr(ci), _np_ptr(vals))
         keep = (rp, ci, vals)
+    if value_type == F32_V8:
+        vt = F32_V8
     h = C.c_void_p()
     st = _stream(stream) if torch.cuda.is_available() else None
     _check(_lib().spc5cuda_mat_create_csr(C.byref(h), vt, nrows, int(ncols), nnz, *ptrs,
@@ -380,14 +392,20 @@ def decode_coo(mat: SPC5Mat, stream=None):
     return rows, cols, vals
 
 
-def beta_matrix(r: int, nrows: int, ncols: int, rowsSize, headers, values, stream=None) -> SPC5Mat:
+def beta_matrix(r: int, nrows: int, ncols: int, rowsSize, headers, values, stream=None,
+                value_type=None) -> SPC5Mat:
     """An ``SPC5Mat`` from already-converted host arrays (e.g. the reference's
-    ``SPC5Mat`` after ``CSR_to_SPC5``)."""
+    ``SPC5Mat`` after ``CSR_to_SPC5``).  ``value_type=F32_V8``: float values
+    with the 8-column headers of the double format."""
     brptr = np.ascontiguousarray(rowsSize, dtype=np.int32)
     hdr = np.ascontiguousarray(headers, dtype=np.uint8)
     vals = np.ascontiguousarray(values)
     vt = _value_type(vals.dtype)
-    stride = 4 + r * (1 if vt == F64 else 2)
+    if value_type == F32_V8:
+        if vals.dtype != np.float32:
+            raise TypeError("F32_V8 values must be float32")
+        vt = F32_V8
+    stride = 4 + r * (2 if vt == F32 else 1)
     if len(hdr) % stride:
         raise ValueError("header array size is not a multiple of the block stride")
     h = C.c_void_p()

@@ -60,9 +60,11 @@ spc5cuda_status spc5cuda_batch_create(spc5cuda_batch** out, int n, spc5cuda_mat*
                 const spc5cuda_mat* m = mats[i];
                 require(m && m->r != 0, SPC5CUDA_ERR_FORMAT, "batch matrices must be converted");
                 require(k[i] >= 0 && ldx[i] >= k[i] && ldy[i] >= k[i], SPC5CUDA_ERR_INVALID, "k");
-                const int kind = mixed ? 2 : (m->value_type == SPC5CUDA_F64 ? 0 : 1);
-                require(!mixed || m->value_type == SPC5CUDA_F32, SPC5CUDA_ERR_FORMAT,
-                        "mixed batches need F32 matrices");
+                const int kind = mixed ? (m->value_type == SPC5CUDA_F32_V8 ? 3 : 2)
+                                       : (m->value_type == SPC5CUDA_F64 ? 0 : 1);
+                require(mixed ? (m->value_type == SPC5CUDA_F32 || m->value_type == SPC5CUDA_F32_V8)
+                              : m->value_type != SPC5CUDA_F32_V8,
+                        SPC5CUDA_ERR_FORMAT, "mixed batches need F32 or F32_V8 matrices, the others F64 or F32");
                 BatchMat& b = hm[size_t(i)];
                 b.brptr = m->brptr.as<int>();
                 b.headers = m->headers.as<uint8_t>();
@@ -135,7 +137,7 @@ spc5cuda_status spc5cuda_batch_create(spc5cuda_batch** out, int n, spc5cuda_mat*
             for (auto& kv : classes) {
                 const int kind = std::get<0>(kv.first), r = std::get<1>(kv.first), kc = std::get<2>(kv.first);
                 const bool staged = std::get<3>(kv.first);
-                const int vs = kind == 0 ? 8 : 16;
+                const int vs = (kind == 0 || kind == 3) ? 8 : 16;
                 const int njobs = int(kv.second.size());
                 const int ctas = std::max(1, std::min(div_up(long(njobs) * vs, 128), sms * 16));
                 SPC5_CUDA(cudaStreamWaitEvent(br[c], fork, 0));

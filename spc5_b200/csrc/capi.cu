@@ -174,7 +174,7 @@ spc5cuda_status spc5cuda_mat_create_csr(spc5cuda_mat** out, int value_type, int 
     return guarded([&] {
         require(out != nullptr, SPC5CUDA_ERR_INVALID, "null out");
         *out = nullptr;
-        require(value_type == SPC5CUDA_F64 || value_type == SPC5CUDA_F32, SPC5CUDA_ERR_INVALID,
+        require(valid_value_type(value_type), SPC5CUDA_ERR_INVALID,
                 "value type");
         require(nrows >= 0 && ncols >= 0 && nnz >= 0 && nnz < (1L << 31), SPC5CUDA_ERR_INVALID,
                 "sizes");
@@ -208,7 +208,7 @@ spc5cuda_status spc5cuda_mat_create_beta(spc5cuda_mat** out, int value_type, int
     return guarded([&] {
         require(out != nullptr, SPC5CUDA_ERR_INVALID, "null out");
         *out = nullptr;
-        require(value_type == SPC5CUDA_F64 || value_type == SPC5CUDA_F32, SPC5CUDA_ERR_INVALID,
+        require(valid_value_type(value_type), SPC5CUDA_ERR_INVALID,
                 "value type");
         require(r_to_format(r) != SPC5CUDA_UNDEFINED_FORMAT, SPC5CUDA_ERR_FORMAT, "r");
         require(nrows >= 0 && ncols >= 0 && nnz >= 0 && nnz < (1L << 31) && nblocks >= 0 &&
@@ -378,6 +378,8 @@ spc5cuda_status spc5cuda_spmv(const spc5cuda_mat* m, const void* x, void* y, voi
         require(m->r != 0, SPC5CUDA_ERR_FORMAT, "SPC5_Spmv : Unknown format type");
         if (m->nrows == 0) return;
         require(x && y, SPC5CUDA_ERR_INVALID, "null vector");
+        require(m->value_type != SPC5CUDA_F32_V8, SPC5CUDA_ERR_FORMAT,
+                "an F32_V8 matrix takes the mixed-precision calls only");
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         if (m->use_plan()) {
             plan_spmv(m, x, y, false, s);
@@ -394,13 +396,15 @@ spc5cuda_status spc5cuda_spmv_mixed(const spc5cuda_mat* m, const float* x, doubl
     return guarded([&] {
         require(m != nullptr, SPC5CUDA_ERR_INVALID, "null");
         require(m->r != 0, SPC5CUDA_ERR_FORMAT, "matrix is not converted");
-        require(m->value_type == SPC5CUDA_F32, SPC5CUDA_ERR_FORMAT,
-                "mixed precision needs an F32 matrix");
+        require(m->value_type == SPC5CUDA_F32 || m->value_type == SPC5CUDA_F32_V8, SPC5CUDA_ERR_FORMAT,
+                "mixed precision needs an F32 or F32_V8 matrix");
         if (m->nrows == 0) return;
         require(x && y, SPC5CUDA_ERR_INVALID, "null vector");
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         if (m->use_plan()) {
             plan_spmv(m, x, y, true, s);
+        } else if (m->value_type == SPC5CUDA_F32_V8) {
+            launch_spmv_mixed8(m->view(), x, y, s);
         } else {
             launch_spmv_mixed(m->view(), x, y, s);
         }
@@ -415,6 +419,8 @@ spc5cuda_status spc5cuda_spmm(const spc5cuda_mat* m, int k, const void* X, long 
         require(k >= 0 && ldx >= k && ldy >= k, SPC5CUDA_ERR_INVALID, "k / leading dimensions");
         if (m->nrows == 0 || k == 0) return;
         require(X && Y, SPC5CUDA_ERR_INVALID, "null block of vectors");
+        require(m->value_type != SPC5CUDA_F32_V8, SPC5CUDA_ERR_FORMAT,
+                "an F32_V8 matrix takes the mixed-precision calls only");
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         if (m->use_plan())
             plan_spmm(m, k, X, ldx, 1, Y, ldy, 1, false, s);
@@ -432,14 +438,16 @@ spc5cuda_status spc5cuda_spmm_mixed(const spc5cuda_mat* m, int k, const float* X
     return guarded([&] {
         require(m != nullptr, SPC5CUDA_ERR_INVALID, "null");
         require(m->r != 0, SPC5CUDA_ERR_FORMAT, "matrix is not converted");
-        require(m->value_type == SPC5CUDA_F32, SPC5CUDA_ERR_FORMAT,
-                "mixed precision needs an F32 matrix");
+        require(m->value_type == SPC5CUDA_F32 || m->value_type == SPC5CUDA_F32_V8, SPC5CUDA_ERR_FORMAT,
+                "mixed precision needs an F32 or F32_V8 matrix");
         require(k >= 0 && ldx >= k && ldy >= k, SPC5CUDA_ERR_INVALID, "k / leading dimensions");
         if (m->nrows == 0 || k == 0) return;
         require(X && Y, SPC5CUDA_ERR_INVALID, "null block of vectors");
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         if (m->use_plan())
             plan_spmm(m, k, X, ldx, 1, Y, ldy, 1, true, s);
+        else if (m->value_type == SPC5CUDA_F32_V8)
+            launch_spmm_mixed8(m->spmm_view(), k, X, ldx, 1, Y, ldy, 1, s);
         else
             launch_spmm_mixed(m->spmm_view(), k, X, ldx, 1, Y, ldy, 1, s);
     });

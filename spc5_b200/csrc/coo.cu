@@ -125,7 +125,7 @@ spc5cuda_status spc5cuda_mat_create_coo(spc5cuda_mat** out, int value_type, int 
     return guarded([&] {
         require(out != nullptr, SPC5CUDA_ERR_INVALID, "null out");
         *out = nullptr;
-        require(value_type == SPC5CUDA_F64 || value_type == SPC5CUDA_F32, SPC5CUDA_ERR_INVALID,
+        require(valid_value_type(value_type), SPC5CUDA_ERR_INVALID,
                 "value type");
         require(nrows >= 0 && ncols >= 0 && nnz >= 0 && nnz < (1L << 31), SPC5CUDA_ERR_INVALID,
                 "sizes");

@@ -90,8 +90,12 @@ inline int r_to_format(int r) {
     }
 }
 
-inline int vs_of(int value_type) { return value_type == SPC5CUDA_F64 ? 8 : 16; }
-inline int mask_bytes_of(int value_type) { return value_type == SPC5CUDA_F64 ? 1 : 2; }
+// F64 and F32_V8 use the 8-column layout (uint8 masks), F32 the 16-column one.
+inline bool valid_value_type(int value_type) {
+    return value_type == SPC5CUDA_F64 || value_type == SPC5CUDA_F32 || value_type == SPC5CUDA_F32_V8;
+}
+inline int vs_of(int value_type) { return value_type == SPC5CUDA_F32 ? 16 : 8; }
+inline int mask_bytes_of(int value_type) { return value_type == SPC5CUDA_F32 ? 2 : 1; }
 inline int value_bytes_of(int value_type) { return value_type == SPC5CUDA_F64 ? 8 : 4; }
 
 template <class F>
@@ -254,9 +258,9 @@ struct spc5cuda_mat {
         spc5cuda::launch_partition(nbr(), brptr.as<int>(), ngroups, gstart.as<int>(), s);
         int max_blocks = 0, max_values = 0;
         spc5cuda::blockrow_max(nbr(), brptr.as<int>(), valptr.as<int>(), &max_blocks, &max_values, s);
-        rows_ok = spc5cuda::rows_fit(vs, r, max_blocks, max_values);
+        rows_ok = spc5cuda::rows_fit(value_type, r, max_blocks, max_values);
         if (rows_ok) {
-            nwarps = spc5cuda::rows_warps(vs, r);
+            nwarps = spc5cuda::rows_warps(value_type, r);
             wstart.alloc(sizeof(int) * size_t(nwarps + 1));
             spc5cuda::launch_partition(nbr(), brptr.as<int>(), nwarps, wstart.as<int>(), s);
         } else {

@@ -75,12 +75,13 @@ void launch_spmv_f64(const BetaView& m, const double* x, double* y, cudaStream_t
 // whether block-rows of at most max_blocks blocks / max_values values fit its
 // staging buffers, and the largest block-row of a converted matrix
 // (synchronises s).
-int rows_warps(int vs, int r, int lanes = 0);
-bool rows_fit(int vs, int r, int max_blocks, int max_values);
+// (vt: the handle's value type, SPC5CUDA_F64 / F32 / F32_V8.)
+int rows_warps(int vt, int r, int lanes = 0);
+bool rows_fit(int vt, int r, int max_blocks, int max_values);
 // Size of a block-row in units of one lane's share of a row-kernel chunk:
 // the block-row fits a chunk of 32 / L block-rows with L lanes each when
 // rows_lane_units(...) <= L * rows_unit().
-long rows_lane_units(int vs, int r, int nblocks, int nvalues);
+long rows_lane_units(int vt, int r, int nblocks, int nvalues);
 long rows_unit();
 // Lanes per block-row of the segmented part of a sorted plan (the largest
 // block-rows), measured on B200 on the N = 4M power-law matrix: more lanes
@@ -95,8 +96,11 @@ void blockrow_max(int nbr, const int* brptr, const int* valptr, int* max_blocks,
 void launch_rows_f64(const BetaView& m, const double* x, double* y, cudaStream_t s);
 void launch_rows_f32(const BetaView& m, const float* x, float* y, cudaStream_t s);
 void launch_rows_mixed(const BetaView& m, const float* x, double* y, cudaStream_t s);
+// Float values in the 8-column layout (F32_V8), float x, FP64 accumulation and y.
+void launch_rows_mixed8(const BetaView& m, const float* x, double* y, cudaStream_t s);
 void launch_spmv_f32(const BetaView& m, const float* x, float* y, cudaStream_t s);
 void launch_spmv_mixed(const BetaView& m, const float* x, double* y, cudaStream_t s);
+void launch_spmv_mixed8(const BetaView& m, const float* x, double* y, cudaStream_t s);
 
 // ---- SpMM (spmm.cu): Y += A X.  Element (row i, right-hand side q) of X
 // is x[i * ldx + q * xcs] (row-major: xcs = 1; column-major: ldx = 1,
@@ -107,6 +111,8 @@ void launch_spmm_f32(const BetaView& m, int k, const float* x, long ldx, long xc
                      long ldy, long ycs, cudaStream_t s);
 void launch_spmm_mixed(const BetaView& m, int k, const float* x, long ldx, long xcs, double* y,
                        long ldy, long ycs, cudaStream_t s);
+void launch_spmm_mixed8(const BetaView& m, int k, const float* x, long ldx, long xcs, double* y,
+                        long ldy, long ycs, cudaStream_t s);
 
 // ---- staged SpMM (spmm_rows.cu) over the per-warp ranges m.wstart /
 // m.nwarps of a matrix whose block-rows fit the row kernels' buffers; same
@@ -117,6 +123,8 @@ void launch_spmm_rows_f32(const BetaView& m, int k, const float* x, long ldx, lo
                           long ldy, long ycs, cudaStream_t s);
 void launch_spmm_rows_mixed(const BetaView& m, int k, const float* x, long ldx, long xcs, double* y,
                             long ldy, long ycs, cudaStream_t s);
+void launch_spmm_rows_mixed8(const BetaView& m, int k, const float* x, long ldx, long xcs, double* y,
+                             long ldy, long ycs, cudaStream_t s);
 
 // ---- batched SpMM (spmm.cu): many matrices, one launch per (r, kc) class
 struct BatchMat {
@@ -141,7 +149,8 @@ struct BatchJob {
 };
 // right-hand sides per pass for rows-per-block r and k right-hand sides
 int batch_kc(int r, int k);
-// kind 0 = f64, 1 = f32, 2 = mixed (f32 values and x, f64 y)
+// kind 0 = f64, 1 = f32, 2 = mixed (f32 values and x, f64 y), 3 = mixed in the
+// 8-column layout (F32_V8 matrices)
 void launch_batch(int kind, int r, int kc, const BatchMat* mats, const BatchJob* jobs, int njobs,
                   int ctas, cudaStream_t s);
 // Right-hand sides per pass of the staged SpMM for VS columns per block,

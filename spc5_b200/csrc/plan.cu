@@ -266,7 +266,7 @@ void build_sorted_plan(spc5cuda_mat* m, cudaStream_t s) {
     DevBuf keys(sizeof(unsigned long long) * size_t(nbr), s), skeys(sizeof(unsigned long long) * size_t(nbr), s);
     DevBuf idx(sizeof(int) * size_t(nbr), s);
     plan->perm.alloc(sizeof(int) * size_t(nbr));
-    const long kb = rows_lane_units(vs, r, 1, 0), kv = rows_lane_units(vs, r, 0, 1);
+    const long kb = rows_lane_units(m->value_type, r, 1, 0), kv = rows_lane_units(m->value_type, r, 0, 1);
     k_row_keys<<<grid_for(nbr, 256), 256, 0, s>>>(nbr, m->brptr.as<int>(), m->valptr.as<int>(), kb, kv,
                                                   keys.as<unsigned long long>(), idx.as<int>());
     SPC5_CUDA(cudaGetLastError());
@@ -356,7 +356,7 @@ void build_sorted_plan(spc5cuda_mat* m, cudaStream_t s) {
             part.nsplit = std::max(1, std::min(spmv_groups(vs, r), rows));
         } else {
             const int per_chunk = 32 / part.lanes;
-            part.nsplit = std::max(1, std::min(rows_warps(vs, r, part.lanes), (rows + per_chunk - 1) / per_chunk));
+            part.nsplit = std::max(1, std::min(rows_warps(m->value_type, r, part.lanes), (rows + per_chunk - 1) / per_chunk));
         }
         part.split.alloc(sizeof(int) * size_t(part.nsplit + 1));
         launch_partition_range(part.a, part.b, plan->sbrptr.as<int>(), part.nsplit, part.split.as<int>(), s);
@@ -432,6 +432,8 @@ void plan_spmv(const spc5cuda_mat* m, const void* x, void* y, bool mixed, cudaSt
     run_parts(m, s, [&](const BetaView& v, cudaStream_t st) {
         if (m->value_type == SPC5CUDA_F64)
             launch_spmv_f64(v, static_cast<const double*>(x), static_cast<double*>(y), st);
+        else if (m->value_type == SPC5CUDA_F32_V8)
+            launch_spmv_mixed8(v, static_cast<const float*>(x), static_cast<double*>(y), st);
         else if (mixed)
             launch_spmv_mixed(v, static_cast<const float*>(x), static_cast<double*>(y), st);
         else
@@ -446,6 +448,9 @@ void plan_spmm(const spc5cuda_mat* m, int k, const void* x, long ldx, long xcs, 
         if (m->value_type == SPC5CUDA_F64)
             launch_spmm_rows_f64(v, k, static_cast<const double*>(x), ldx, xcs, static_cast<double*>(y), ldy, ycs,
                                  st);
+        else if (m->value_type == SPC5CUDA_F32_V8)
+            launch_spmm_rows_mixed8(v, k, static_cast<const float*>(x), ldx, xcs, static_cast<double*>(y), ldy,
+                                    ycs, st);
         else if (mixed)
             launch_spmm_rows_mixed(v, k, static_cast<const float*>(x), ldx, xcs, static_cast<double*>(y), ldy, ycs,
                                    st);

@@ -155,6 +155,9 @@ bool spc5cuda_server::dispatch(Slot& sl) {
         SPC5_CUDA(cudaMemsetAsync(y0, 0, size_t(m->nrows) * yb, sl.stream));
         if (m->use_plan())
             plan_spmv(m, io[0].first, y0, cfg.mixed, sl.stream);
+        else if (cfg.mixed && m->value_type == SPC5CUDA_F32_V8)
+            launch_spmv_mixed8(m->view(), static_cast<const float*>(io[0].first), static_cast<double*>(y0),
+                               sl.stream);
         else if (cfg.mixed)
             launch_spmv_mixed(m->view(), static_cast<const float*>(io[0].first), static_cast<double*>(y0),
                               sl.stream);
@@ -171,6 +174,9 @@ bool spc5cuda_server::dispatch(Slot& sl) {
     SPC5_CUDA(cudaMemsetAsync(Y, 0, size_t(k) * ldY * yb, sl.stream));
     if (m->use_plan())
         plan_spmm(m, k, X, 1, ldX, Y, 1, ldY, cfg.mixed, sl.stream);
+    else if (cfg.mixed && m->value_type == SPC5CUDA_F32_V8)
+        launch_spmm_mixed8(m->spmm_view(), k, reinterpret_cast<const float*>(X), 1, ldX,
+                           reinterpret_cast<double*>(Y), 1, ldY, sl.stream);
     else if (cfg.mixed)
         launch_spmm_mixed(m->spmm_view(), k, reinterpret_cast<const float*>(X), 1, ldX,
                           reinterpret_cast<double*>(Y), 1, ldY, sl.stream);
@@ -265,7 +271,8 @@ spc5cuda_status spc5cuda_server_add_matrix(spc5cuda_server* sv, spc5cuda_mat* m,
     return guarded([&] {
         require(sv && m && id, SPC5CUDA_ERR_INVALID, "null");
         require(m->r != 0, SPC5CUDA_ERR_FORMAT, "served matrices must be converted");
-        require(sv->cfg.mixed ? m->value_type == SPC5CUDA_F32 : m->value_type == SPC5CUDA_F64,
+        require(sv->cfg.mixed ? (m->value_type == SPC5CUDA_F32 || m->value_type == SPC5CUDA_F32_V8)
+                              : m->value_type == SPC5CUDA_F64,
                 SPC5CUDA_ERR_FORMAT, "value type does not match the server");
         std::unique_lock<std::mutex> lk(sv->mu);
         require(sv->inflight == 0, SPC5CUDA_ERR_INVALID, "add matrices while the server is idle");

@@ -267,6 +267,12 @@ void launch_spmm_mixed(const BetaView& m, int k, const float* x, long ldx, long 
     launch_spmm_impl<float, float, float, double, double>(m, k, x, ldx, xcs, y, ldy, ycs, s);
 }
 
+void launch_spmm_mixed8(const BetaView& m, int k, const float* x, long ldx, long xcs, double* y,
+                        long ldy, long ycs, cudaStream_t s) {
+    if (m.wstart) return launch_spmm_rows_mixed8(m, k, x, ldx, xcs, y, ldy, ycs, s);
+    launch_spmm_impl<double, float, float, double, double>(m, k, x, ldx, xcs, y, ldy, ycs, s);
+}
+
 int batch_kc(int r, int k) {
     const int kmax = r >= 8 ? 4 : (r >= 4 ? 8 : 16);
     int kc = 1;
@@ -316,8 +322,10 @@ void launch_batch(int kind, int r, int kc, const BatchMat* mats, const BatchJob*
         batch_impl<double, double, double, double, double>(r, kc, mats, jobs, njobs, ctas, s);
     else if (kind == 1)
         batch_impl<float, float, float, float, float>(r, kc, mats, jobs, njobs, ctas, s);
-    else
+    else if (kind == 2)
         batch_impl<float, float, float, double, double>(r, kc, mats, jobs, njobs, ctas, s);
+    else
+        batch_impl<double, float, float, double, double>(r, kc, mats, jobs, njobs, ctas, s);
     SPC5_CUDA(cudaGetLastError());
 }
 

@@ -368,6 +368,11 @@ void launch_spmm_rows_mixed(const BetaView& m, int k, const float* x, long ldx, 
     spmm_rows_impl<float, float, float, double, double>(m, k, x, ldx, xcs, y, ldy, ycs, s);
 }
 
+void launch_spmm_rows_mixed8(const BetaView& m, int k, const float* x, long ldx, long xcs, double* y, long ldy,
+                             long ycs, cudaStream_t s) {
+    spmm_rows_impl<double, float, float, double, double>(m, k, x, ldx, xcs, y, ldy, ycs, s);
+}
+
 void launch_batch_rows(int kind, int r, int kc, const BatchMat* mats, const BatchJob* jobs, int njobs,
                        cudaStream_t s) {
     if (njobs <= 0) return;
@@ -376,8 +381,10 @@ void launch_batch_rows(int kind, int r, int kc, const BatchMat* mats, const Batc
         batch_rows_impl<double, double, double, double, double>(r, kc, mats, jobs, njobs, ctas, s);
     else if (kind == 1)
         batch_rows_impl<float, float, float, float, float>(r, kc, mats, jobs, njobs, ctas, s);
-    else
+    else if (kind == 2)
         batch_rows_impl<float, float, float, double, double>(r, kc, mats, jobs, njobs, ctas, s);
+    else
+        batch_rows_impl<double, float, float, double, double>(r, kc, mats, jobs, njobs, ctas, s);
     SPC5_CUDA(cudaGetLastError());
 }
 

@@ -596,4 +596,9 @@ void launch_spmv_mixed(const BetaView& m, const float* x, double* y, cudaStream_
     else launch_impl<float, float, float, double, double>(m, x, y, s);
 }
 
+void launch_spmv_mixed8(const BetaView& m, const float* x, double* y, cudaStream_t s) {
+    if (m.wstart) launch_rows_mixed8(m, x, y, s);
+    else launch_impl<double, float, float, double, double>(m, x, y, s);
+}
+
 }  // namespace spc5cuda

@@ -369,10 +369,12 @@ __global__ void k_blockrow_max(int nbr, const int* __restrict__ brptr, const int
 
 }  // namespace
 
-int rows_warps(int vs, int r, int lanes) {
+int rows_warps(int vt, int r, int lanes) {
     int per_sm;
-    if (vs == 8) {
+    if (vt == SPC5CUDA_F64) {
         per_sm = rows_occupancy<double, double, double, double, double>(r, lanes);
+    } else if (vt == SPC5CUDA_F32_V8) {
+        per_sm = rows_occupancy<double, float, float, double, double>(r, lanes);
     } else {
         per_sm = std::min(rows_occupancy<float, float, float, float, float>(r, lanes),
                           rows_occupancy<float, float, float, double, double>(r, lanes));
@@ -384,20 +386,20 @@ int rows_warps(int vs, int r, int lanes) {
 constexpr int ROWS_HB = rows::HB;
 constexpr int ROWS_VB = rows::VB;
 
-bool rows_fit(int vs, int r, int max_blocks, int max_values) {
+bool rows_fit(int vt, int r, int max_blocks, int max_values) {
     // every block-row alone must fit the staging buffers, alignment included
-    const int stride = 4 + r * (vs == 8 ? 1 : 2);
-    const int vbytes = vs == 8 ? 8 : 4;
+    const int stride = 4 + r * (vt == SPC5CUDA_F32 ? 2 : 1);
+    const int vbytes = vt == SPC5CUDA_F64 ? 8 : 4;
     const long hneed = long(max_blocks) * stride + 32;
     const long vneed = (long(max_values) + 2 * (16 / vbytes)) * vbytes;
     return hneed <= ROWS_HB && vneed <= ROWS_VB;
 }
 
-long rows_lane_units(int vs, int r, int nblocks, int nvalues) {
+long rows_lane_units(int vt, int r, int nblocks, int nvalues) {
     // a block-row of this size fits `lanes` lanes' share of a chunk (32 / lanes
     // block-rows per chunk) when the result is <= lanes * ROWS_UNIT
-    const long stride = 4 + r * (vs == 8 ? 1 : 2);
-    const long vbytes = vs == 8 ? 8 : 4;
+    const long stride = 4 + r * (vt == SPC5CUDA_F32 ? 2 : 1);
+    const long vbytes = vt == SPC5CUDA_F64 ? 8 : 4;
     return std::max(long(nblocks) * stride * (ROWS_VB - 32), long(nvalues) * vbytes * (ROWS_HB - 32));
 }
 
@@ -435,6 +437,10 @@ void launch_rows_f32(const BetaView& m, const float* x, float* y, cudaStream_t s
 
 void launch_rows_mixed(const BetaView& m, const float* x, double* y, cudaStream_t s) {
     launch_rows_impl<float, float, float, double, double>(m, x, y, s);
+}
+
+void launch_rows_mixed8(const BetaView& m, const float* x, double* y, cudaStream_t s) {
+    launch_rows_impl<double, float, float, double, double>(m, x, y, s);
 }
 
 }  // namespace spc5cuda

@@ -55,13 +55,14 @@ double measure_us(const spc5cuda_mat* m, int r, cudaStream_t s) {
     const int ngroups = spmv_groups(vs, r);
     DevBuf gstart(sizeof(int) * size_t(ngroups + 1), s);
     DevBuf x(vb * size_t(m->ncols) + 16, s);
-    DevBuf y(vb * size_t(m->nrows) + 16, s);
+    const size_t yb = m->value_type == SPC5CUDA_F32_V8 ? 8 : vb;  // F32_V8: FP64 y
+    DevBuf y(yb * size_t(m->nrows) + 16, s);
     launch_emit(vs, r, m->nrows, m->rowptr.as<int>(), m->colidx.as<int>(), m->values.p, int(vb),
                 brptr.as<int>(), headers.as<uint8_t>(), values.p, s);
     launch_valptr_from_csr(r, m->nrows, m->rowptr.as<int>(), valptr.as<int>(), s);
     launch_partition(nbr, brptr.as<int>(), ngroups, gstart.as<int>(), s);
     SPC5_CUDA(cudaMemsetAsync(x.p, 0, vb * size_t(m->ncols) + 16, s));
-    SPC5_CUDA(cudaMemsetAsync(y.p, 0, vb * size_t(m->nrows) + 16, s));
+    SPC5_CUDA(cudaMemsetAsync(y.p, 0, yb * size_t(m->nrows) + 16, s));
     BetaView v;
     v.r = r;
     v.nrows = m->nrows;
@@ -75,6 +76,8 @@ double measure_us(const spc5cuda_mat* m, int r, cudaStream_t s) {
     auto run = [&] {
         if (m->value_type == SPC5CUDA_F64)
             launch_spmv_f64(v, x.as<double>(), y.as<double>(), s);
+        else if (m->value_type == SPC5CUDA_F32_V8)
+            launch_spmv_mixed8(v, x.as<float>(), y.as<double>(), s);
         else
             launch_spmv_f32(v, x.as<float>(), y.as<float>(), s);
     };
@@ -121,7 +124,8 @@ spc5cuda_status spc5cuda_find_best(const spc5cuda_mat* m, int* r_out, double* es
         for (int f = 0; f < 3; ++f) {
             DevBuf tmp(sizeof(int) * size_t(div_up(m->nrows, rs[f]) + 1), s);
             const long nb = m->nrows > 0 ? count_blocks(m, rs[f], tmp.as<int>(), s) : 0;
-            const double* c = m->value_type == SPC5CUDA_F64 ? cd[f] : cf[f];
+            // the double model for the 8-column layouts (F64, F32_V8)
+            const double* c = m->value_type == SPC5CUDA_F32 ? cf[f] : cd[f];
             const double avg = double(m->nnz) / double(nb);
             const double speed = c[0] * (avg * avg * avg) + c[1] * (avg * avg) + c[2] * avg + c[3];
             if (speed > best_speed) {

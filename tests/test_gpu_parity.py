@@ -239,6 +239,62 @@ def test_mixed_precision(cuda, r):
             assert (np.abs(y - y64) / np.maximum(absrow, 1e-300)).max() <= 2.5e-7
 
 
+@pytest.mark.parametrize("r", [1, 2, 4, 8])
+def test_mixed_precision_v8_layout(cuda, r):
+    """F32_V8: float values in the 8-column layout.  Arrays equal the double
+    conversion with values rounded to float; y equals the FP64 oracle on the
+    widened values and x bit for bit (row kernel and sorted plan), and is
+    within 1e-6 normwise of the FP64 CSR result on the unrounded inputs."""
+    cases = list(irregular_cases()) + [M.powerlaw(60000, seed=5), M.stencil27(20)]
+    for csr in cases:
+        m = S.csr_matrix(csr.rowptr, csr.colidx, csr.values, csr.ncols, value_type=S.F32_V8)
+        S.CSR_to_SPC5(m, S.FORMAT_OF_R[r])
+        assert m.value_type == S.F32_V8 and m.info().vs == 8
+        ob, oh, ov = oracle.csr_to_beta_v8(r, csr.rowptr, csr.colidx, csr.values)
+        gb, gh, gv = m.arrays()
+        assert np.array_equal(gb, ob) and np.array_equal(gh, oh) and gv.tobytes() == ov.tobytes(), csr.name
+        x = M.x_vector(csr.ncols, 5)
+        x32 = x.astype(np.float32)
+        y0 = M.x_vector(csr.nrows, 6)
+        y = dev(y0)
+        for _ in range(3):
+            S.SPC5_Spmv_mixed(m, dev(x32), y)
+        torch.cuda.synchronize()
+        yo = y0.copy()
+        for _ in range(3):
+            oracle.beta_spmv_mixed8(r, csr.nrows, ob, oh, ov, x32, yo)
+        assert y.cpu().numpy().tobytes() == yo.tobytes(), csr.name
+        if csr.nnz:
+            y1 = torch.zeros(csr.nrows, dtype=torch.float64, device="cuda")
+            S.SPC5_Spmv_mixed(m, dev(x32), y1)
+            y1 = y1.cpu().numpy()
+            y64, absrow = oracle.csr_spmv_f64(csr.rowptr, csr.colidx, csr.values, x, np.zeros(csr.nrows))
+            assert np.abs(y1 - y64).max() / np.abs(y64).max() <= 1e-6
+            assert (np.abs(y1 - y64) / np.maximum(absrow, 1e-300)).max() <= 2.5e-7
+    # the plain calls reject the layout
+    with pytest.raises(S.SPC5Error):
+        S.SPC5_Spmv(m, dev(x32), dev(np.zeros(csr.nrows, np.float32)))
+
+
+@pytest.mark.parametrize("r", [1, 4])
+def test_mixed_v8_spmm_columns_equal_oracle(cuda, r):
+    """Mixed SpMM on an F32_V8 matrix: every column equals the oracle's mixed
+    SpMV of that column (staged SpMM and the sorted plan's SpMM)."""
+    for csr in (M.banded(3000, 40, 0.2, seed=9), M.powerlaw(30000, seed=4)):
+        m = S.csr_matrix(csr.rowptr, csr.colidx, csr.values, csr.ncols, value_type=S.F32_V8)
+        S.CSR_to_SPC5(m, S.FORMAT_OF_R[r])
+        ob, oh, ov = oracle.csr_to_beta_v8(r, csr.rowptr, csr.colidx, csr.values)
+        k = 5
+        X = np.stack([M.x_vector(csr.ncols, 20 + j).astype(np.float32) for j in range(k)], axis=1)
+        Y = torch.zeros((csr.nrows, k), dtype=torch.float64, device="cuda")
+        S.SPC5_Spmm_mixed(m, torch.from_numpy(np.ascontiguousarray(X)).cuda(), Y)
+        torch.cuda.synchronize()
+        Yh = Y.cpu().numpy()
+        for j in range(k):
+            yo = oracle.beta_spmv_mixed8(r, csr.nrows, ob, oh, ov, X[:, j].copy(), np.zeros(csr.nrows))
+            assert Yh[:, j].tobytes() == yo.tobytes(), (csr.name, j)
+
+
 def test_fp64_matches_csr_oracle_componentwise(cuda):
     csr = M.powerlaw(50000, seed=2)
     x = M.x_vector(csr.ncols, 6)
