@@ -208,34 +208,27 @@ class ClockSampler:
 # CPU baseline: the reference's OpenMP path
 # ---------------------------------------------------------------------------
 
-def cpu_baseline(csr, budget_s=20.0, formats=FORMATS):
-    """Times SPC5_{r}rVc_Spmv_omp of the compiled reference on this host.
-    Returns (GB/s, cores, description) over a bounded number of steps."""
-    import oracle
-    if not (oracle.ref_available() and oracle.cpu_has_avx512()):
+def cpu_baseline_subprocess(args, steps=16):
+    """The reference's own AVX-512 OpenMP SpMV on this host, run as the
+    reference arm in a separate process (``bench.py --impl reference``) with
+    all host threads and nothing else running: {value, unit, cores, kind,
+    sample}, or None when the reference is not available here."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference", "--workload", args.workload,
+           "--steps", str(steps), "--warmup", "1", "--formats", ",".join(str(r) for r in FORMATS),
+           "--gpus", "1"]
+    if args.size is not None:
+        cmd += ["--size", str(args.size)]
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    try:
+        res = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env)
+        line = json.loads(res.stdout.strip().splitlines()[-1])
+    except Exception:
         return None
-    threads = oracle.ref().ref_max_threads()
-    xp = oracle.x_padded(M.x_vector(csr.ncols, 0))
-    mats, total_bytes = [], 0
-    for r in formats:
-        m = oracle.RefMatrix(csr.rowptr, csr.colidx, csr.values, csr.ncols)
-        nb = m.convert(r)
-        m.split(threads)
-        mats.append(m)
-        total_bytes += spmv_bytes(csr.nnz, nb, r, csr.nrows, csr.ncols)
-    y = np.zeros(csr.nrows + 8)
-    for m in mats:  # warm-up
-        m.time_spmv_omp(xp, y, 1)
-    t0 = time.perf_counter()
-    steps, secs = 0, 0.0
-    while secs < budget_s and steps < 64:
-        for m in mats:
-            secs += m.time_spmv_omp(xp, y, 1)
-        steps += 1
-        if time.perf_counter() - t0 > 2 * budget_s:
-            break
-    gbs = total_bytes * steps / secs / 1e9
-    return gbs, threads, steps, secs
+    if "unavailable" in line:
+        return None
+    cpu = dict(line["cpu_baseline"])
+    cpu["sample"] += "; separate process (bench.py --impl reference), before the GPU legs"
+    return cpu
 
 
 def run_reference(args):
@@ -253,13 +246,15 @@ def run_reference(args):
     csr = build_workload(args.workload, args.size)
     threads = oracle.ref().ref_max_threads()
     xp = oracle.x_padded(M.x_vector(csr.ncols, 0))
-    mats, step_bytes = [], 0
+    mats, step_bytes, blocks, bytes_of = [], 0, {}, []
     for r in FORMATS:
         m = oracle.RefMatrix(csr.rowptr, csr.colidx, csr.values, csr.ncols)
         nb = m.convert(r)
         m.split(threads)
         mats.append(m)
-        step_bytes += spmv_bytes(csr.nnz, nb, r, csr.nrows, csr.ncols)
+        blocks[r] = nb
+        bytes_of.append(spmv_bytes(csr.nnz, nb, r, csr.nrows, csr.ncols))
+        step_bytes += bytes_of[-1]
     y = np.zeros(csr.nrows + 8)
     for _ in range(args.warmup):
         for m in mats:
@@ -273,8 +268,8 @@ def run_reference(args):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(secs / args.steps * 1e3, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "desc": workload_desc(args.workload, csr),
-                       "formats": list(FORMATS), "l2": "inputs larger than L2"},
+            "config": spmv_config(args.workload, csr, blocks, args.gpus,
+                                  L2_NOTE_FLUSH if min(bytes_of) < L2_BYTES else L2_NOTE_LARGE),
             "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": "reference",
                              "sample": f"{args.steps} steps x {len(FORMATS)} SPC5_Spmv_omp calls (r={FORMATS}) on the "
                                        f"full matrix, OMP threads={threads}"},
@@ -349,33 +344,25 @@ def mixed_legs(csr, mats, x, per_r_ms, args, stream, select_kernel):
     return res
 
 
-def run_gpu(args):
+def spmv_config(workload, csr, blocks, nranks, l2_note):
+    """The ``config`` dict of an SpMV line, identical in both arms."""
+    return {"workload": workload, "desc": workload_desc(workload, csr), "formats": list(FORMATS),
+            "nrows": csr.nrows, "nnz": csr.nnz, "blocks": {str(r): int(blocks[r]) for r in FORMATS},
+            "l2": l2_note, "parallelism": f"replica per GPU x{nranks}"}
+
+
+L2_NOTE_LARGE = "inputs larger than L2 (every matrix > 126 MB, read in turn)"
+L2_NOTE_FLUSH = "L2 flushed (256 MB write) before every SpMV; value from the SpMVs' own CUDA events"
+
+
+def spmv_leg(csr, args, dev, world, barrier, max_over_ranks, steps, warmup, e2e=True, mixed=True):
+    """One SpMV workload on this GPU: every format converted on the device,
+    then the device-timed steps (one y += A x per format), per-format GB/s,
+    the launch-level roofline, the end-to-end rate through the public API with
+    host buffers, and the mixed-precision legs."""
     import torch
-    import torch.distributed as dist
 
     import spc5_b200 as S
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    csr = build_workload(args.workload, args.size)
     stream = torch.cuda.current_stream()
     mats, bytes_of = [], {}
     for r in FORMATS:
@@ -403,19 +390,19 @@ def run_gpu(args):
             if events is not None:
                 events[i][1].record(stream)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     torch.cuda.synchronize()
 
     # ---- device-timed region (inputs resident, larger than L2) ----
     launch_ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-                  for _ in mats] for _ in range(args.steps)]
+                  for _ in mats] for _ in range(steps)]
     t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
+    with ClockSampler(dev.index) as clk:
         barrier()
         torch.cuda.synchronize()
         t_start.record(stream)
-        for k in range(args.steps):
+        for k in range(steps):
             step(launch_ev[k])
         t_end.record(stream)
         clk.sample_now()  # the queued steps are still running
@@ -423,13 +410,13 @@ def run_gpu(args):
         barrier()
     clocks = clk.summary()
     ms_local = t_start.elapsed_time(t_end)
-    per_r_ms = {r: statistics.mean(launch_ev[k][i][0].elapsed_time(launch_ev[k][i][1]) for k in range(args.steps))
+    per_r_ms = {r: statistics.mean(launch_ev[k][i][0].elapsed_time(launch_ev[k][i][1]) for k in range(steps))
                 for i, (r, _) in enumerate(mats)}
     kernel_ms = sum(per_r_ms.values())
     if flush is not None:
-        ms_local = kernel_ms * args.steps  # the SpMVs without the flushes between them
+        ms_local = kernel_ms * steps  # the SpMVs without the flushes between them
     ms = max_over_ranks(ms_local)
-    value = step_bytes * args.steps * world / (ms * 1e-3) / 1e9
+    value = step_bytes * steps * world / (ms * 1e-3) / 1e9
     warm = None
     if flush is not None:
         # the same steps back to back without flushes: the matrices stay in L2
@@ -437,107 +424,166 @@ def run_gpu(args):
         torch.cuda.synchronize()
         w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         w0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             step(cold=False)
         w1.record(stream)
         torch.cuda.synchronize()
         wms = max_over_ranks(w0.elapsed_time(w1))
-        warm = {"value": round(step_bytes * args.steps * world / (wms * 1e-3) / 1e9, 2), "unit": UNIT,
+        warm = {"value": round(step_bytes * steps * world / (wms * 1e-3) / 1e9, 2), "unit": UNIT,
                 "note": "no L2 flush between SpMVs: the matrices stay in L2"}
     achieved = step_bytes / (kernel_ms * 1e-3) / 1e9
     peak, peak_kind = load_peaks()
+    out = {"value": value, "ms": ms, "step_bytes": step_bytes, "mats": mats, "x": x, "y": y,
+           "blocks": {r: m.numberOfBlocks for r, m in mats}, "flush": flush is not None,
+           "per_format_gbs": {str(r): round(bytes_of[r] / (per_r_ms[r] * 1e-3) / 1e9, 2) for r in FORMATS},
+           "per_r_ms": per_r_ms, "bytes_of": bytes_of, "achieved": achieved, "peak": peak,
+           "peak_kind": peak_kind, "clocks": clocks, "warm": warm,
+           "gflops": 2 * csr.nnz * len(FORMATS) * steps * world / (ms * 1e-3) / 1e9}
 
-    # ---- e2e through the public API with host buffers ----
-    # Every step copies its own x and y in from pinned host memory, runs the
-    # SpMVs and copies its y back.  Steps alternate between two streams with
-    # their own device and host buffers, so one step's copies overlap the
-    # previous step's kernels (what a caller streaming requests does).
-    x_host = torch.from_numpy(M.x_vector(csr.ncols, 0)).pin_memory()
-    e2e_streams = [torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)]
-    e2e_bufs = [(torch.empty_like(x), torch.empty_like(y),
-                 torch.zeros(csr.nrows, dtype=torch.float64).pin_memory(),
-                 torch.zeros(csr.nrows, dtype=torch.float64).pin_memory()) for _ in range(2)]
+    if e2e:
+        # ---- e2e through the public API with host buffers ----
+        # Every step copies its own x and y in from pinned host memory, runs
+        # the SpMVs and copies its y back.  Steps alternate between two
+        # streams with their own device and host buffers, so one step's copies
+        # overlap the previous step's kernels (what a caller streaming
+        # requests does).
+        x_host = torch.from_numpy(M.x_vector(csr.ncols, 0)).pin_memory()
+        e2e_streams = [torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)]
+        e2e_bufs = [(torch.empty_like(x), torch.empty_like(y),
+                     torch.zeros(csr.nrows, dtype=torch.float64).pin_memory(),
+                     torch.zeros(csr.nrows, dtype=torch.float64).pin_memory()) for _ in range(2)]
 
-    def e2e_step(k):
-        xd, yd, yh_in, yh_out = e2e_bufs[k % 2]
-        with torch.cuda.stream(e2e_streams[k % 2]):
-            xd.copy_(x_host, non_blocking=True)
-            yd.copy_(yh_in, non_blocking=True)
-            for r, m in mats:
-                S.SPC5_Spmv(m, xd, yd)
-            yh_out.copy_(yd, non_blocking=True)
+        def e2e_step(k):
+            xd, yd, yh_in, yh_out = e2e_bufs[k % 2]
+            with torch.cuda.stream(e2e_streams[k % 2]):
+                xd.copy_(x_host, non_blocking=True)
+                yd.copy_(yh_in, non_blocking=True)
+                for r, m in mats:
+                    S.SPC5_Spmv(m, xd, yd)
+                yh_out.copy_(yd, non_blocking=True)
 
-    for k in range(max(1, args.warmup)):
-        e2e_step(k)
-    torch.cuda.synchronize()
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for st in e2e_streams:
-        st.wait_event(e0)
-    for k in range(args.steps):
-        e2e_step(k)
-    for st in e2e_streams:
-        stream.wait_stream(st)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
-    e2e_value = step_bytes * args.steps * world / (e2e_ms * 1e-3) / 1e9
+        for k in range(max(1, warmup)):
+            e2e_step(k)
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for st in e2e_streams:
+            st.wait_event(e0)
+        for k in range(steps):
+            e2e_step(k)
+        for st in e2e_streams:
+            stream.wait_stream(st)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+        out["e2e"] = {"value": round(step_bytes * steps * world / (e2e_ms * 1e-3) / 1e9, 2), "unit": UNIT,
+                      "h2d_bytes_per_step": int(x.numel() * 8 + y.numel() * 8),
+                      "d2h_bytes_per_step": int(y.numel() * 8)}
 
     # ---- mixed precision on the same matrix: float values and x, FP64
     # accumulation and y, in the 8-column layout (F32_V8, the default) and in
     # the reference's float layout (beta(r,16)); the error is stated against an
     # FP64 CSR product of the unrounded matrix and x on the device (cuSPARSE
     # through torch), per row relative to sum_j |a_ij x_j| and normwise
-    mixed = {}
-    if not args.no_mixed:
-        mixed = mixed_legs(csr, mats, x, per_r_ms, args, stream, select_kernel)
+    out["mixed"] = {}
+    if mixed:
+        a2 = argparse.Namespace(**vars(args))
+        a2.steps, a2.warmup = steps, warmup
+        out["mixed"] = mixed_legs(csr, mats, x, per_r_ms, a2, stream, select_kernel)
+    return out
 
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    # the CPU baseline first, in its own process, before this process touches
+    # the GPU (rank 0 at N = 1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_subprocess(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    csr = build_workload(args.workload, args.size)
+    main = spmv_leg(csr, args, dev, world, barrier, max_over_ranks, args.steps, args.warmup,
+                    mixed=not args.no_mixed)
+    mats = main["mats"]
     traffic, traffic_src = args.traffic, "ncu (given)" if args.traffic else None
     ratios = TRAFFIC_RATIO.get(args.workload)
     if traffic is None and ratios and args.kernel == "auto" and all(r in ratios for r in FORMATS):
-        traffic = int(sum(ratios[r] * bytes_of[r] for r in FORMATS))
+        traffic = int(sum(ratios[r] * main["bytes_of"][r] for r in FORMATS))
         traffic_src = "ncu DRAM bytes per algorithmic byte at a smaller size of the same generator, scaled"
     line = None
     if rank == 0:
-        cpu = None
-        if not args.no_cpu_baseline:
-            res = cpu_baseline(csr, formats=FORMATS)
-            if res is not None:
-                gbs, threads, nsteps, secs = res
-                cpu = {"value": round(gbs, 3), "unit": UNIT, "cores": threads, "kind": "reference",
-                       "sample": f"{nsteps} steps x {len(FORMATS)} SPC5_Spmv_omp (r={list(FORMATS)}) on the full matrix, "
-                                 f"{secs:.1f} s"}
         line = {
-            "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+            "metric": METRIC, "value": round(main["value"], 2), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(main["ms"] / args.steps, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": args.workload, "desc": workload_desc(args.workload, csr),
-                       "formats": list(FORMATS), "nrows": csr.nrows, "nnz": csr.nnz,
-                       "blocks": {str(r): m.numberOfBlocks for r, m in mats},
-                       "l2": ("inputs larger than L2 (every matrix > 126 MB, read in turn)" if flush is None
-                              else "L2 flushed (256 MB write) before every SpMV; value from the SpMVs' own "
-                                   "CUDA events"),
-                       "parallelism": f"replica per GPU x{world}"},
-            "per_format_gbs": {str(r): round(bytes_of[r] / (per_r_ms[r] * 1e-3) / 1e9, 2) for r in FORMATS},
-            "gflops": round(2 * csr.nnz * len(FORMATS) * args.steps * world / (ms * 1e-3) / 1e9, 2),
-            "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                         "traffic": traffic,
-                         "traffic_source": traffic_src,
+            "config": spmv_config(args.workload, csr, main["blocks"], world,
+                                  L2_NOTE_FLUSH if main["flush"] else L2_NOTE_LARGE),
+            "per_format_gbs": main["per_format_gbs"],
+            "gflops": round(main["gflops"], 2),
+            "roofline": {"bound": "hbm", "achieved": round(main["achieved"], 2), "peak": main["peak"],
+                         "unit": "GB/s", "frac": round(main["achieved"] / main["peak"], 4),
+                         "peak_kind": main["peak_kind"], "traffic": traffic, "traffic_source": traffic_src,
                          "kernel": ", ".join(sorted({KERNEL_NAME[m.kernel] for _, m in mats}))},
             "kernels": {str(r): KERNEL_NAME[m.kernel] for r, m in mats},
-            "e2e": {"value": round(e2e_value, 2), "unit": UNIT,
-                    "h2d_bytes_per_step": int(x.numel() * 8 + y.numel() * 8),
-                    "d2h_bytes_per_step": int(y.numel() * 8)},
+            "e2e": main["e2e"],
             "gpu_launches": sum(m.spmv_launches for _, m in mats) * args.steps,
-            "clocks": clocks,
-            "mixed": mixed,
-            "cpu_baseline": cpu,
+            "clocks": main["clocks"],
+            "mixed": main["mixed"],
         }
-        if warm is not None:
-            line["warm"] = warm
+        if main["warm"] is not None:
+            line["warm"] = main["warm"]
+    del main, mats
+    torch.cuda.empty_cache()
+    # ---- the other configurations of the metric, on this GPU (N = 1 only):
+    # the 27-point stencil 160^3 (FP64 vs mixed), the 5-point Poisson 512^2
+    # (L2-resident: cold and warm) and a short serving run
+    if world == 1 and args.workload == "powerlaw" and args.size is None and not args.no_extra:
+        extra_steps, extra_warm = max(5, args.steps // 2), 3
+        for name, key in (("stencil27", "config3_stencil27_160"), ("poisson", "config1_poisson_512")):
+            c2 = build_workload(name)
+            leg = spmv_leg(c2, args, dev, world, barrier, max_over_ranks, extra_steps, extra_warm,
+                           e2e=False, mixed=(name == "stencil27" and not args.no_mixed))
+            entry = {"value": round(leg["value"], 2), "unit": UNIT, "steps": extra_steps,
+                     "config": spmv_config(name, c2, leg["blocks"], world,
+                                           L2_NOTE_FLUSH if leg["flush"] else L2_NOTE_LARGE),
+                     "per_format_gbs": leg["per_format_gbs"],
+                     "roofline_frac": round(leg["achieved"] / leg["peak"], 4),
+                     "kernels": {str(r): KERNEL_NAME[m.kernel] for r, m in leg["mats"]},
+                     "clocks": leg["clocks"]}
+            if leg["mixed"]:
+                entry["mixed"] = leg["mixed"]
+            if leg["warm"] is not None:
+                entry["warm"] = leg["warm"]
+            line[key] = entry
+            line["gpu_launches"] += sum(m.spmv_launches for _, m in leg["mats"]) * extra_steps
+            del leg, c2
+            torch.cuda.empty_cache()
+        line["config5_serving"] = serve_leg(args, rates=(5000.0, 50000.0), seconds=1.0, precisions=(False,))
+    if rank == 0:
+        line["cpu_baseline"] = cpu
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -638,15 +684,16 @@ def serve_pool():
             M.powerlaw(2_000_000, seed=24), M.stencil27(126)]
 
 
-def run_serve(args):
+def serve_leg(args, rates, seconds, precisions=(False, True)):
+    """The request loop over the 64-matrix pool at each offered rate (Poisson
+    arrivals, Zipf(1.1) matrix choice) for each precision (False: FP64, True:
+    mixed in the 8-column layout); one result dict per (precision, rate)."""
     import torch
 
     import spc5_b200 as S
-    torch.cuda.set_device(0)
     distinct = serve_pool()
-    rates = [float(t) for t in args.rates.split(",")]
     results = []
-    for mixed in (False, True):
+    for mixed in precisions:
         dt = np.float32 if mixed else np.float64
         tdt = torch.float32 if mixed else torch.float64
         mats = []
@@ -683,7 +730,7 @@ def run_serve(args):
         zipf_w /= zipf_w.sum()
         for rate in rates:
             rng = np.random.default_rng(int(rate))
-            nreq = int(rate * args.serve_seconds)
+            nreq = int(rate * seconds)
             arrivals = np.cumsum(rng.exponential(1.0 / rate, size=nreq))
             choice = rng.choice(len(mats), size=nreq, p=zipf_w)
             srv.stats(reset=True)
@@ -710,6 +757,14 @@ def run_serve(args):
         srv.close()
         del mats, ybufs, xs
         torch.cuda.empty_cache()
+    return results
+
+
+def run_serve(args):
+    import torch
+    torch.cuda.set_device(0)
+    rates = [float(t) for t in args.rates.split(",")]
+    results = serve_leg(args, rates, args.serve_seconds)
     best = max(r["req_per_s"] for r in results if r["precision"] == "f64")
     line = {"metric": "served SpMV req/s and p50/p99 latency", "value": best, "unit": "req/s",
             "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -770,6 +825,8 @@ def main():
     ap.add_argument("--formats", default="1,2,4,8", help="comma list of r to run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="default run: skip the stencil, Poisson and serving legs")
     ap.add_argument("--kernel", choices=["auto", "groups", "rows", "sorted"], default="auto",
                     help="SpMV kernel (rows falls back to auto where a block-row does not fit)")
     ap.add_argument("--traffic", type=float, default=None,

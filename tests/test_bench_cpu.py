@@ -29,11 +29,30 @@ def test_reference_arm_prints_one_json_line():
 
 
 @needs_ref
-def test_cpu_baseline_helper():
+def test_cpu_baseline_runs_the_reference_arm_in_a_subprocess():
+    sys.path.insert(0, ROOT)
+    import argparse
+    import bench
+    args = argparse.Namespace(workload="powerlaw", size=20000)
+    cpu = bench.cpu_baseline_subprocess(args, steps=2)
+    assert cpu is not None
+    assert cpu["kind"] == "reference" and cpu["value"] > 0 and cpu["cores"] >= 1
+    assert "separate process" in cpu["sample"]
+
+
+@needs_ref
+def test_reference_arm_config_matches_the_gpu_arm():
+    """The reference arm's config dict is built by the same helper as the GPU
+    arm's, from the same conversion block counts."""
     sys.path.insert(0, ROOT)
     import bench
-    from spc5_b200 import matrices as M
-    res = bench.cpu_baseline(M.poisson2d(64), budget_s=0.2, formats=(1, 4))
-    assert res is not None
-    gbs, threads, steps, secs = res
-    assert gbs > 0 and threads >= 1 and steps >= 1 and secs > 0
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                          "--size", "20000", "--steps", "1", "--warmup", "1"],
+                         capture_output=True, text=True, timeout=600, cwd=ROOT)
+    d = json.loads(out.stdout.strip().splitlines()[-1])
+    csr = bench.build_workload("powerlaw", 20000)
+    blocks = {r: oracle.block_count(r, csr.rowptr, csr.colidx) for r in bench.FORMATS}
+    want = bench.spmv_config("powerlaw", csr, blocks, 1, bench.L2_NOTE_LARGE if
+                             min(bench.spmv_bytes(csr.nnz, blocks[r], r, csr.nrows, csr.ncols)
+                                 for r in bench.FORMATS) >= bench.L2_BYTES else bench.L2_NOTE_FLUSH)
+    assert d["config"] == json.loads(json.dumps(want))
