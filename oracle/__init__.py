@@ -31,12 +31,22 @@ _L = C.c_long
 _D = C.c_double
 
 
+def ref_src() -> str:
+    """The reference's ``src/`` directory: ``$REF_SRC``, else the default of
+    oracle/Makefile (the one place that names it)."""
+    env = os.environ.get("REF_SRC")
+    if env:
+        return env
+    out = subprocess.run(["make", "-s", "-C", HERE, "print-ref-src"], capture_output=True, text=True)
+    return out.stdout.strip()
+
+
 def build(ref: bool = True) -> None:
     """Compile liboracle.so, and _ref/libspc5ref.so when the reference sources exist."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    ref_src = os.environ.get("REF_SRC", "/root/reference/src")
-    if ref and os.path.exists(os.path.join(ref_src, "spc5.hpp")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_SRC={ref_src}"], check=True)
+    src = ref_src()
+    if ref and src and os.path.exists(os.path.join(src, "spc5.hpp")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_SRC={src}"], check=True)
 
 
 def _ptr(a):

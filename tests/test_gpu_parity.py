@@ -338,8 +338,7 @@ def test_full_size_bit_exact(cuda, which):
     bit-identical to the oracle, for every r."""
     csr = M.powerlaw() if which == "powerlaw" else M.stencil27(160)
     x = M.x_vector(csr.ncols, 0)
-    rs = (1, 2, 4, 8) if which == "powerlaw" else (4,)
-    for r in rs:
+    for r in (1, 2, 4, 8):
         brptr, headers, ov = oracle.csr_to_beta(r, csr.rowptr, csr.colidx, csr.values)
         m = converted(csr, np.float64, r)
         gb, gh, gv = m.arrays()
@@ -348,6 +347,81 @@ def test_full_size_bit_exact(cuda, which):
         y = gpu_spmv(m, x, np.zeros(csr.nrows))
         assert y.tobytes() == yo.tobytes()
         del m
+
+
+@pytest.mark.slow
+def test_full_size_poisson_512(cuda):
+    """The 5-point Poisson 512^2 workload (beta(2,8) is its headline format,
+    every r is checked): conversion byte-identical and FP64 y bit-identical to
+    the oracle's AVX-512 order, and componentwise within 1e-13 of the FP64
+    scalar CSR product (CSR_Spmv_scalar, src/spc5.hpp:116-127)."""
+    csr = M.poisson2d(512)
+    x = M.x_vector(csr.ncols, 0)
+    y64, absrow = oracle.csr_spmv_f64(csr.rowptr, csr.colidx, csr.values, x, np.zeros(csr.nrows))
+    for r in (2, 1, 4, 8):
+        brptr, headers, ov = oracle.csr_to_beta(r, csr.rowptr, csr.colidx, csr.values)
+        m = converted(csr, np.float64, r)
+        gb, gh, gv = m.arrays()
+        assert np.array_equal(gb, brptr) and np.array_equal(gh, headers) and gv.tobytes() == ov.tobytes()
+        y0 = M.x_vector(csr.nrows, 9)
+        yo = oracle.beta_spmv_f64(r, csr.nrows, brptr, headers, ov, x, y0.copy())
+        assert gpu_spmv(m, x, y0).tobytes() == yo.tobytes()
+        y = gpu_spmv(m, x, np.zeros(csr.nrows))
+        assert (np.abs(y - y64) / np.maximum(absrow, 1e-300)).max() <= 1e-13
+
+
+@pytest.mark.slow
+def test_full_size_stencil_f32_and_mixed(cuda):
+    """The 27-point stencil 160^3 in the float layouts: FP32 (beta(r,16))
+    and mixed bit-identical to the oracle, in the reference's float layout and
+    in the 8-column layout; the mixed results within 1e-6 normwise and 2.5e-7
+    per row (relative to sum_j |a_ij x_j|) of the FP64 CSR product."""
+    csr = M.stencil27(160)
+    x = M.x_vector(csr.ncols, 0)
+    x32 = x.astype(np.float32)
+    y64, absrow = oracle.csr_spmv_f64(csr.rowptr, csr.colidx, csr.values, x, np.zeros(csr.nrows))
+
+    def close(y):
+        assert np.abs(y - y64).max() / np.abs(y64).max() <= 1e-6
+        assert (np.abs(y - y64) / np.maximum(absrow, 1e-300)).max() <= 2.5e-7
+
+    r = 4
+    v32 = csr.values.astype(np.float32)
+    brptr, headers, ov = oracle.csr_to_beta(r, csr.rowptr, csr.colidx, v32)
+    m = converted(csr, np.float32, r)
+    gb, gh, gv = m.arrays()
+    assert np.array_equal(gb, brptr) and np.array_equal(gh, headers) and gv.tobytes() == ov.tobytes()
+    yf = dev(np.zeros(csr.nrows, np.float32))
+    S.SPC5_Spmv(m, dev(x32), yf)
+    yo = oracle.beta_spmv_f32(r, csr.nrows, brptr, headers, ov, x32, np.zeros(csr.nrows, np.float32))
+    assert yf.cpu().numpy().tobytes() == yo.tobytes()
+    ym = torch.zeros(csr.nrows, dtype=torch.float64, device="cuda")
+    S.SPC5_Spmv_mixed(m, dev(x32), ym)
+    torch.cuda.synchronize()
+    ym = ym.cpu().numpy()
+    assert ym.tobytes() == oracle.beta_spmv_mixed(r, csr.nrows, brptr, headers, ov, x32,
+                                                  np.zeros(csr.nrows)).tobytes()
+    close(ym)
+    del m
+    for r in (1, 4):
+        b8, h8, v8 = oracle.csr_to_beta_v8(r, csr.rowptr, csr.colidx, csr.values)
+        m8 = S.csr_matrix(csr.rowptr, csr.colidx, csr.values, csr.ncols, value_type=S.F32_V8)
+        S.CSR_to_SPC5(m8, S.FORMAT_OF_R[r])
+        gb, gh, gv = m8.arrays()
+        assert np.array_equal(gb, b8) and np.array_equal(gh, h8) and gv.tobytes() == v8.tobytes()
+        y8 = torch.zeros(csr.nrows, dtype=torch.float64, device="cuda")
+        S.SPC5_Spmv_mixed(m8, dev(x32), y8)
+        torch.cuda.synchronize()
+        y8 = y8.cpu().numpy()
+        assert y8.tobytes() == oracle.beta_spmv_mixed8(r, csr.nrows, b8, h8, v8, x32, np.zeros(csr.nrows)).tobytes()
+        close(y8)
+        del m8
+
+
+def oracle_spmv(dt, r, nrows, brptr, headers, vals, x, y):
+    """The oracle's y += A x for the value type of the arrays."""
+    f = oracle.beta_spmv_f64 if dt == np.float64 else oracle.beta_spmv_f32
+    return f(r, nrows, brptr, headers, vals, x, y)
 
 
 @pytest.mark.parametrize("tag,dt", DTYPES)
@@ -364,8 +438,10 @@ def test_spmm_columns_equal_spmv(cuda, tag, dt, r, k):
         S.SPC5_Spmm(m, dev(X), Yd)
         torch.cuda.synchronize()
         Y = Yd.cpu().numpy()
+        brptr, headers, ov = oracle.csr_to_beta(r, csr.rowptr, csr.colidx, csr.values.astype(dt))
         for j in range(k):
-            yj = gpu_spmv(m, np.ascontiguousarray(X[:, j]), np.ascontiguousarray(Y0[:, j]))
+            yj = oracle_spmv(dt, r, csr.nrows, brptr, headers, ov, np.ascontiguousarray(X[:, j]),
+                             np.ascontiguousarray(Y0[:, j]))
             assert Y[:, j].tobytes() == yj.tobytes(), (csr.name, j)
 
 
@@ -448,7 +524,8 @@ def test_autotune(cuda, mode):
 @pytest.mark.parametrize("mixed", [False, True])
 def test_batch_equals_independent_spmv(cuda, mixed):
     """One graph over matrices of uneven sizes, r and k: every column equals
-    the independent SpMV bit for bit."""
+    the oracle's SpMV bit for bit (mixed: F32 and F32_V8 matrices in one
+    batch)."""
     rng = np.random.default_rng(5)
     mats, Xs, Ys, keep = [], [], [], []
     dt = np.float32 if mixed else np.float64
@@ -457,22 +534,33 @@ def test_batch_equals_independent_spmv(cuda, mixed):
         csr = M.banded(n, int(rng.integers(2, 60)), 0.3, seed=100 + i)
         r = (1, 2, 4, 8)[i % 4]
         k = (1, 4, 8, 16, 3)[i % 5]
-        m = converted(csr, dt, r)
+        v8 = mixed and i % 2 == 1
+        if v8:
+            m = S.csr_matrix(csr.rowptr, csr.colidx, csr.values, csr.ncols, value_type=S.F32_V8)
+            S.CSR_to_SPC5(m, S.FORMAT_OF_R[r])
+        else:
+            m = converted(csr, dt, r)
         X = dev(np.stack([M.x_vector(n, 200 + i * 20 + j, dt) for j in range(k)], axis=1))
         Y = torch.zeros(n, k, dtype=torch.float64 if mixed or dt == np.float64 else torch.float32,
                         device="cuda")
-        mats.append(m); Xs.append(X); Ys.append(Y); keep.append((csr, r))
+        mats.append(m); Xs.append(X); Ys.append(Y); keep.append((csr, r, v8))
     b = S.Batch(mats, Xs, Ys, mixed=mixed)
     nclasses, njobs = b.info()
     assert nclasses >= 4 and njobs >= 12
     for _ in range(2):  # y accumulates over two replays
         b.launch()
     torch.cuda.synchronize()
-    for m, X, Y, (csr, r) in zip(mats, Xs, Ys, keep):
+    for m, X, Y, (csr, r, v8) in zip(mats, Xs, Ys, keep):
+        brptr, headers, vals = m.arrays()
+        Xh, Yh = X.cpu().numpy(), Y.cpu().numpy()
         for j in range(X.shape[1]):
-            y = torch.zeros(csr.nrows, dtype=Y.dtype, device="cuda")
-            xj = X[:, j].contiguous()
+            xj = np.ascontiguousarray(Xh[:, j])
+            y = np.zeros(csr.nrows, dtype=Yh.dtype)
             for _ in range(2):
-                (S.SPC5_Spmv_mixed if mixed else S.SPC5_Spmv)(m, xj, y)
-            torch.cuda.synchronize()
-            assert Y[:, j].cpu().numpy().tobytes() == y.cpu().numpy().tobytes(), (csr.name, r, j)
+                if v8:
+                    oracle.beta_spmv_mixed8(r, csr.nrows, brptr, headers, vals, xj, y)
+                elif mixed:
+                    oracle.beta_spmv_mixed(r, csr.nrows, brptr, headers, vals, xj, y)
+                else:
+                    oracle_spmv(dt, r, csr.nrows, brptr, headers, vals, xj, y)
+            assert Yh[:, j].tobytes() == y.tobytes(), (csr.name, r, j)

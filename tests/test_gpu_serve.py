@@ -28,12 +28,20 @@ def solo(m, x, mixed):
     return y
 
 
-@pytest.mark.parametrize("mixed", [False, True])
-def test_results_same_alone_and_in_the_mix(cuda, mixed):
+@pytest.mark.parametrize("vt", [S.F64, S.F32, S.F32_V8])
+def test_results_same_alone_and_in_the_mix(cuda, vt):
+    mixed = vt != S.F64
     dt = np.float32 if mixed else np.float64
     tdt = torch.float32 if mixed else torch.float64
     csrs = [M.powerlaw(20000, seed=3), M.stencil27(18), M.banded(7000, 40, 0.2, seed=5)]
-    mats = [converted(c, dt, r) for c, r in zip(csrs, (1, 4, 2))]
+    if vt == S.F32_V8:
+        mats = []
+        for c, r in zip(csrs, (1, 4, 2)):
+            m = S.csr_matrix(c.rowptr, c.colidx, c.values, c.ncols, value_type=S.F32_V8)
+            S.CSR_to_SPC5(m, S.FORMAT_OF_R[r])
+            mats.append(m)
+    else:
+        mats = [converted(c, dt, r) for c, r in zip(csrs, (1, 4, 2))]
     srv = S.Server(slots=3, max_k=16, mixed=mixed)
     ids = [srv.add_matrix(m) for m in mats]
     rng = np.random.default_rng(0)
@@ -60,6 +68,36 @@ def test_results_same_alone_and_in_the_mix(cuda, mixed):
         assert y2.cpu().numpy().tobytes() == y.cpu().numpy().tobytes()
     srv.close()
     del tdt
+
+
+def test_bounded_wait_times_out_then_drains(cuda):
+    """wait() with a zero timeout on a request queued behind work returns
+    SPC5CUDA_ERR_TIMEOUT (6) without touching the request; drain() then
+    completes everything and the result equals a solo SpMV.  No device
+    spin: the timeout is on the host's wait for the completion event."""
+    csr = M.powerlaw(400_000, seed=12)
+    m = converted(csr, np.float64, 1)
+    srv = S.Server(slots=1, max_k=16)
+    mid = srv.add_matrix(m)
+    x = torch.from_numpy(M.x_vector(csr.ncols, 77)).cuda()
+    timed_out = False
+    for burst in (64, 256, 1024):
+        ys = [torch.zeros(csr.nrows, dtype=torch.float64, device="cuda") for _ in range(burst)]
+        torch.cuda.synchronize()
+        rids = [srv.submit(mid, x, y) for y in ys]
+        try:
+            srv.wait(rids[-1], timeout_s=0.0)
+        except S.SPC5Error as e:
+            assert e.status == 6
+            timed_out = True
+        srv.drain(timeout_s=120.0)
+        ref = solo(m, x, False).cpu().numpy().tobytes()
+        assert ys[-1].cpu().numpy().tobytes() == ref and ys[0].cpu().numpy().tobytes() == ref
+        del ys
+        if timed_out:
+            break
+    assert timed_out
+    srv.close()
 
 
 def test_admission_by_hbm_footprint(cuda):
