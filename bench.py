@@ -355,7 +355,40 @@ L2_NOTE_LARGE = "inputs larger than L2 (every matrix > 126 MB, read in turn)"
 L2_NOTE_FLUSH = "L2 flushed (256 MB write) before every SpMV; value from the SpMVs' own CUDA events"
 
 
-def spmv_leg(csr, args, dev, world, barrier, max_over_ranks, steps, warmup, e2e=True, mixed=True):
+def dropin_leg(mats, csr, x, steps, warmup, stream):
+    """The reference-named void symbols core_SPC5_{r}rVc_Spmv_double over
+    device copies of the converted arrays (no handle): per call the library
+    derives the block-row offsets and splits on the device and runs the row
+    kernel when every block-row fits it, else the group kernel."""
+    import torch
+
+    import spc5_b200 as S
+    per, total_bytes, total_ms = {}, 0, 0.0
+    y = torch.zeros(csr.nrows, dtype=torch.float64, device=x.device)
+    for r, m in mats:
+        b, h, v = m.arrays()
+        bd, hd, vd = (torch.from_numpy(a).to(x.device) for a in (b, h, v))
+        for _ in range(warmup):
+            S.core_spmv_void(r, csr.nrows, bd, hd, vd, x, y, stream)
+        torch.cuda.synchronize()
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(steps):
+            S.core_spmv_void(r, csr.nrows, bd, hd, vd, x, y, stream)
+        e.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(e) / steps
+        nbytes = spmv_bytes(csr.nnz, m.numberOfBlocks, r, csr.nrows, csr.ncols)
+        per[str(r)] = round(nbytes / (ms * 1e-3) / 1e9, 2)
+        total_bytes += nbytes
+        total_ms += ms
+        del bd, hd, vd
+    return {"value": round(total_bytes / (total_ms * 1e-3) / 1e9, 2), "unit": UNIT, "per_format_gbs": per,
+            "call": "core_SPC5_{r}rVc_Spmv_double (void, reference argument list, device pointers)"}
+
+
+def spmv_leg(csr, args, dev, world, barrier, max_over_ranks, steps, warmup, e2e=True, mixed=True,
+             dropin=False):
     """One SpMV workload on this GPU: every format converted on the device,
     then the device-timed steps (one y += A x per format), per-format GB/s,
     the launch-level roofline, the end-to-end rate through the public API with
@@ -481,6 +514,9 @@ def spmv_leg(csr, args, dev, world, barrier, max_over_ranks, steps, warmup, e2e=
                       "h2d_bytes_per_step": int(x.numel() * 8 + y.numel() * 8),
                       "d2h_bytes_per_step": int(y.numel() * 8)}
 
+    if dropin:
+        out["dropin"] = dropin_leg(mats, csr, x, steps, warmup, stream)
+
     # ---- mixed precision on the same matrix: float values and x, FP64
     # accumulation and y, in the 8-column layout (F32_V8, the default) and in
     # the reference's float layout (beta(r,16)); the error is stated against an
@@ -525,7 +561,7 @@ def run_gpu(args):
 
     csr = build_workload(args.workload, args.size)
     main = spmv_leg(csr, args, dev, world, barrier, max_over_ranks, args.steps, args.warmup,
-                    mixed=not args.no_mixed)
+                    mixed=not args.no_mixed, dropin=(world == 1 and not args.no_extra))
     mats = main["mats"]
     traffic, traffic_src = args.traffic, "ncu (given)" if args.traffic else None
     ratios = TRAFFIC_RATIO.get(args.workload)
@@ -553,6 +589,8 @@ def run_gpu(args):
             "clocks": main["clocks"],
             "mixed": main["mixed"],
         }
+        if "dropin" in main:
+            line["dropin"] = main["dropin"]
         if main["warm"] is not None:
             line["warm"] = main["warm"]
     del main, mats
@@ -565,7 +603,8 @@ def run_gpu(args):
         for name, key in (("stencil27", "config3_stencil27_160"), ("poisson", "config1_poisson_512")):
             c2 = build_workload(name)
             leg = spmv_leg(c2, args, dev, world, barrier, max_over_ranks, extra_steps, extra_warm,
-                           e2e=False, mixed=(name == "stencil27" and not args.no_mixed))
+                           e2e=False, mixed=(name == "stencil27" and not args.no_mixed),
+                           dropin=(name == "stencil27"))
             entry = {"value": round(leg["value"], 2), "unit": UNIT, "steps": extra_steps,
                      "config": spmv_config(name, c2, leg["blocks"], world,
                                            L2_NOTE_FLUSH if leg["flush"] else L2_NOTE_LARGE),
@@ -575,6 +614,8 @@ def run_gpu(args):
                      "clocks": leg["clocks"]}
             if leg["mixed"]:
                 entry["mixed"] = leg["mixed"]
+            if "dropin" in leg:
+                entry["dropin"] = leg["dropin"]
             if leg["warm"] is not None:
                 entry["warm"] = leg["warm"]
             line[key] = entry

@@ -78,6 +78,53 @@ void spc5cuda::valptr_from_headers(int mask_bytes, int r, int nbr, const int* br
 
 namespace {
 
+// The library's own stream-ordered memory pool on the current device: the
+// per-call scratch of the drop-in symbols comes from it, and it keeps freed
+// memory for the next call (release threshold: never), so repeated calls do
+// not go back to the driver.  One pool per device for the process lifetime.
+cudaMemPool_t scratch_pool() {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    SPC5_CUDA(cudaGetDevice(&dev));
+    require(dev >= 0 && dev < 64, SPC5CUDA_ERR_UNSUPPORTED, "device index");
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pools[dev]) {
+        cudaMemPoolProps props;
+        std::memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        SPC5_CUDA(cudaMemPoolCreate(&pools[dev], &props));
+        uint64_t keep = UINT64_MAX;
+        SPC5_CUDA(cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep));
+    }
+    return pools[dev];
+}
+
+// Stream-ordered scratch from scratch_pool().
+struct PoolBuf {
+    void* p = nullptr;
+    cudaStream_t s;
+    PoolBuf(size_t n, cudaStream_t st) : s(st) {
+        SPC5_CUDA(cudaMallocFromPoolAsync(&p, std::max<size_t>(n, 16), scratch_pool(), st));
+    }
+    ~PoolBuf() {
+        if (p) cudaFreeAsync(p, s);
+    }
+    PoolBuf(const PoolBuf&) = delete;
+    PoolBuf& operator=(const PoolBuf&) = delete;
+    template <class U>
+    U* as() const { return static_cast<U*>(p); }
+};
+
+// core_SPC5_{r}rVc_Spmv_{double,float} over device arrays without a handle.
+// Per call, all on the stream and without a host round trip: the value
+// offsets of the block-rows (one pass over the headers), the largest
+// block-row, the per-group and per-warp splits; then the row kernel and the
+// group kernel are both enqueued, gated on a device word: the row kernel runs
+// when every block-row fits its staging buffers, the group kernel otherwise.
+// Both give the reference's bits.
 template <class T>
 void core_spmv(int r, long nbRows, const int* rowsSizes, const unsigned char* headers,
                const T* values, const T* x, T* y, cudaStream_t s) {
@@ -88,12 +135,22 @@ void core_spmv(int r, long nbRows, const int* rowsSizes, const unsigned char* he
     require(rowsSizes && x && y, SPC5CUDA_ERR_INVALID, "null pointer");
     require(aligned(headers, 4) && aligned(values, 16) && aligned(rowsSizes, 4),
             SPC5CUDA_ERR_INVALID, "misaligned array (headers 4 bytes, values 16 bytes)");
+    constexpr int vt = sizeof(T) == 8 ? SPC5CUDA_F64 : SPC5CUDA_F32;
     const int nbr = div_up(nbRows, r);
-    const int ngroups = spmv_groups(sizeof(T) == 8 ? 8 : 16, r);
-    DevBuf valptr(sizeof(int) * size_t(nbr + 1), s);
-    DevBuf gstart(sizeof(int) * size_t(ngroups + 1), s);
-    valptr_from_headers(sizeof(T) == 8 ? 1 : 2, r, nbr, rowsSizes, headers, valptr.as<int>(), s);
+    const int ngroups = spmv_groups(vs_of(vt), r);
+    const int nwarps = rows_warps(vt, r);
+    PoolBuf valptr(sizeof(int) * size_t(nbr + 1), s);
+    PoolBuf gstart(sizeof(int) * size_t(ngroups + 1), s);
+    PoolBuf wstart(sizeof(int) * size_t(nwarps + 1), s);
+    PoolBuf work(sizeof(int) * 4, s);
+    {
+        PoolBuf tmp(sizeof(int) * size_t(scan_tmp_ints(nbr) + 1), s);
+        launch_blockrow_value_counts(mask_bytes_of(vt), r, nbr, rowsSizes, headers, valptr.as<int>(), s);
+        exclusive_scan_i32(valptr.as<int>(), valptr.as<int>(), nbr, tmp.as<int>(), s);
+    }
     launch_partition(nbr, rowsSizes, ngroups, gstart.as<int>(), s);
+    launch_partition(nbr, rowsSizes, nwarps, wstart.as<int>(), s);
+    launch_rows_fit_flag(vt, r, nbr, rowsSizes, valptr.as<int>(), work.as<int>(), s);
     BetaView v;
     v.r = r;
     v.nrows = int(nbRows);
@@ -104,10 +161,19 @@ void core_spmv(int r, long nbRows, const int* rowsSizes, const unsigned char* he
     v.valptr = valptr.as<int>();
     v.gstart = gstart.as<int>();
     v.ngroups = ngroups;
-    if constexpr (sizeof(T) == 8)
+    v.run_if = work.as<int>();
+    BetaView vr = v;
+    vr.wstart = wstart.as<int>();
+    vr.nwarps = nwarps;
+    v.run_if_value = 0;   // group kernel: some block-row does not fit
+    vr.run_if_value = 1;  // row kernel: every block-row fits
+    if constexpr (sizeof(T) == 8) {
+        launch_spmv_f64(vr, x, y, s);
         launch_spmv_f64(v, x, y, s);
-    else
+    } else {
+        launch_spmv_f32(vr, x, y, s);
         launch_spmv_f32(v, x, y, s);
+    }
 }
 
 }  // namespace

@@ -58,6 +58,10 @@ struct BetaView {
     // block-row of y for each block-row of these arrays (null: the same);
     // set when the arrays are a reordered copy of the matrix
     const int* perm = nullptr;
+    // when set, the launch does its work only if *run_if == run_if_value (a
+    // device word written by an earlier kernel on the same stream)
+    const int* run_if = nullptr;
+    int run_if_value = 0;
 };
 
 // Number of VS-lane groups the SpMV kernels launch on the current device
@@ -93,6 +97,11 @@ int rows_hb();
 int rows_vb();
 void blockrow_max(int nbr, const int* brptr, const int* valptr, int* max_blocks, int* max_values,
                   cudaStream_t s);
+// The same test on the device, without a host round trip: work[0] = 1 when
+// every block-row fits the row kernel's buffers, else 0 (work holds 3 ints;
+// work[1], work[2] receive the largest block and value counts).
+void launch_rows_fit_flag(int vt, int r, int nbr, const int* brptr, const int* valptr, int* work,
+                          cudaStream_t s);
 void launch_rows_f64(const BetaView& m, const double* x, double* y, cudaStream_t s);
 void launch_rows_f32(const BetaView& m, const float* x, float* y, cudaStream_t s);
 void launch_rows_mixed(const BetaView& m, const float* x, double* y, cudaStream_t s);

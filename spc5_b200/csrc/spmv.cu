@@ -33,6 +33,9 @@
 // slot in shared memory; the slots of a window are reduced together at its
 // end, one lane per (block-row, sub-row), with the same tree.
 #include <climits>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -193,7 +196,10 @@ __global__ void __launch_bounds__(128)
     k_spmv(int nrows, const int* __restrict__ brptr, const uint8_t* __restrict__ headers,
            const V* __restrict__ values, const int* __restrict__ valptr,
            const int* __restrict__ gstart, int ngroups, const int* __restrict__ perm,
-           const X* __restrict__ x, Y* __restrict__ y) {
+           const X* __restrict__ x, Y* __restrict__ y, const int* __restrict__ run_if, int run_if_value) {
+    // a launch gated on a device word: the drop-in symbols enqueue the row
+    // kernel and this one, and exactly one of them does the work
+    if (run_if && __ldg(run_if) != run_if_value) return;
     using G = Geo<LT, R, V, A>;
     using F = Fields<G::MB>;
     constexpr int VS = G::VS, MW = G::MW, NW = G::NW, PW = F::PER_WORD;
@@ -503,7 +509,8 @@ void launch_impl(const BetaView& m, const X* x, Y* y, cudaStream_t s) {
         auto kern = k_spmv<LT, R_, V, X, A, Y>;                                                  \
         set_smem(kern, G::SMEM);                                                                 \
         kern<<<ctas, G::THREADS, G::SMEM, s>>>(m.nrows, m.brptr, m.headers, vals, m.valptr,      \
-                                               m.gstart, m.ngroups, m.perm, x, y);               \
+                                               m.gstart, m.ngroups, m.perm, x, y, m.run_if,      \
+                                               m.run_if_value);                                  \
     }
     switch (m.r) {
         case 1: SPC5_LAUNCH(1); break;
@@ -553,7 +560,18 @@ int groups_per_cta(int) {
 }  // namespace
 
 int spmv_groups(int vs, int r) {
-    // one wave of resident CTAs: the static partition then has no tail
+    // one wave of resident CTAs: the static partition then has no tail;
+    // cached per (device, VS, r) (the drop-in symbols ask on every call)
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int>, int> cache;
+    int dev = 0;
+    SPC5_CUDA(cudaGetDevice(&dev));
+    const auto key = std::make_tuple(dev, vs, r);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
     int per_sm, gpc;
     if (vs == 8) {
         per_sm = occupancy<double, double, double, double, double>(r);
@@ -564,7 +582,10 @@ int spmv_groups(int vs, int r) {
         gpc = groups_per_cta<float, float>(r);
     }
     per_sm = std::max(1, std::min(per_sm, SPMV_CTAS_PER_SM));
-    return sm_count() * per_sm * gpc;
+    const int n = sm_count() * per_sm * gpc;
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = n;
+    return n;
 }
 
 void launch_partition(int nbr, const int* brptr, int ngroups, int* gstart, cudaStream_t s) {

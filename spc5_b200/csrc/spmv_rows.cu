@@ -26,8 +26,11 @@
 // accumulator unchanged for finite x (it starts at +0.0 and never becomes
 // -0.0), so y is bit-identical for finite x.
 #include <algorithm>
-#include <type_traits>
 #include <climits>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <type_traits>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -122,7 +125,9 @@ __global__ void __launch_bounds__(ROWS_THREADS)
     k_rows(int nrows, const int* __restrict__ brptr, const uint8_t* __restrict__ headers,
            const V* __restrict__ values, const int* __restrict__ valptr,
            const int* __restrict__ wstart, int nwarps, const int* __restrict__ perm, int nseg,
-           const X* __restrict__ x, Y* __restrict__ y) {
+           const X* __restrict__ x, Y* __restrict__ y, const int* __restrict__ run_if, int run_if_value) {
+    // a launch gated on a device word (see BetaView::run_if)
+    if (run_if && __ldg(run_if) != run_if_value) return;
     using G = RowGeo<LT, R, V, L>;
     constexpr int VS = G::VS, MB = G::MB, MW = G::MW, SPW = G::SPW;
     constexpr int FPW = 4 / MB;  // mask fields per 32-bit word
@@ -344,9 +349,18 @@ void launch_rows_impl(const BetaView& m, const X* x, Y* y, cudaStream_t s) {
         auto kern = m.nseg > 0 ? k_rows<LT, R_, V, X, A, Y, L_, true> : k_rows<LT, R_, V, X, A, Y, L_, false>;
         set_smem(kern, G::SMEM);
         kern<<<ctas, ROWS_THREADS, G::SMEM, s>>>(m.nrows, m.brptr, m.headers, vals, m.valptr, m.wstart,
-                                                 m.nwarps, m.perm, m.nseg, x, y);
+                                                 m.nwarps, m.perm, m.nseg, x, y, m.run_if, m.run_if_value);
     });
     SPC5_CUDA(cudaGetLastError());
+}
+
+// flag[0] = 1 when a block-row of maxes[0] blocks and maxes[1] values fits
+// the staging buffers (the test of rows_fit, on the device), else 0.
+__global__ void k_fit_flag(const int* __restrict__ maxes, int stride, int vbytes, int hb, int vb,
+                           int* __restrict__ flag) {
+    const long hneed = long(maxes[0]) * stride + 32;
+    const long vneed = (long(maxes[1]) + 2 * (16 / vbytes)) * vbytes;
+    flag[0] = (hneed <= hb && vneed <= vb) ? 1 : 0;
 }
 
 // Largest block count and value count of any block-row.
@@ -370,6 +384,18 @@ __global__ void k_blockrow_max(int nbr, const int* __restrict__ brptr, const int
 }  // namespace
 
 int rows_warps(int vt, int r, int lanes) {
+    // cached per (device, value type, r, lanes): the drop-in symbols ask on
+    // every call
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int, int>, int> cache;
+    int dev = 0;
+    SPC5_CUDA(cudaGetDevice(&dev));
+    const auto key = std::make_tuple(dev, vt, r, lanes);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
     int per_sm;
     if (vt == SPC5CUDA_F64) {
         per_sm = rows_occupancy<double, double, double, double, double>(r, lanes);
@@ -379,7 +405,10 @@ int rows_warps(int vt, int r, int lanes) {
         per_sm = std::min(rows_occupancy<float, float, float, float, float>(r, lanes),
                           rows_occupancy<float, float, float, double, double>(r, lanes));
     }
-    return sm_count() * per_sm * ROWS_WARPS;
+    const int n = sm_count() * per_sm * ROWS_WARPS;
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = n;
+    return n;
 }
 
 // Staging buffer sizes of RowGeo (every instantiation).
@@ -425,6 +454,21 @@ void blockrow_max(int nbr, const int* brptr, const int* valptr, int* max_blocks,
     SPC5_CUDA(cudaStreamSynchronize(s));
     *max_blocks = h[0];
     *max_values = h[1];
+}
+
+void launch_rows_fit_flag(int vt, int r, int nbr, const int* brptr, const int* valptr, int* work,
+                          cudaStream_t s) {
+    SPC5_CUDA(cudaMemsetAsync(work, 0, 3 * sizeof(int), s));
+    if (nbr > 0) {
+        const int threads = 256;
+        const int blocks = std::max(1, std::min(div_up(nbr, threads), sm_count() * 4));
+        k_blockrow_max<<<blocks, threads, 0, s>>>(nbr, brptr, valptr, work + 1);
+        SPC5_CUDA(cudaGetLastError());
+    }
+    const int stride = 4 + r * (vt == SPC5CUDA_F32 ? 2 : 1);
+    const int vbytes = vt == SPC5CUDA_F64 ? 8 : 4;
+    k_fit_flag<<<1, 1, 0, s>>>(work + 1, stride, vbytes, ROWS_HB, ROWS_VB, work);
+    SPC5_CUDA(cudaGetLastError());
 }
 
 void launch_rows_f64(const BetaView& m, const double* x, double* y, cudaStream_t s) {

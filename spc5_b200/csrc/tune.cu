@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <memory>
 
 #include "handle.h"
 
@@ -11,75 +12,80 @@ namespace spc5cuda {
 
 namespace {
 
-// Algorithmic bytes of one y += A x in beta(r,VS) (values, headers, block-row
-// pointer, x once, y read and written).
-double spmv_bytes(const spc5cuda_mat* m, int r, long nblocks) {
-    const double sv = value_bytes_of(m->value_type);
-    const double mb = mask_bytes_of(m->value_type);
-    const double nbr = double(div_up(m->nrows, r));
-    return double(m->nnz) * sv + double(nblocks) * (4.0 + r * mb) + 4.0 * (nbr + 1.0) +
-           double(m->ncols) * sv + 2.0 * double(m->nrows) * sv;
-}
-
-// B200 cost model of the SpMV kernel (spmv.cu): the kernel is bounded by
-// whichever is slower, streaming its algorithmic bytes at the sustained
-// fraction of HBM bandwidth it reaches, or issuing its per-block work.  The
-// per-block costs are SpMV times measured on a B200 (148 SMs, 1.965 GHz)
-// divided by the block count, on a 27-point stencil and a power-law matrix;
-// the f32 layout has twice the lanes per block.
-constexpr double kHbmBytesPerUs = 6.0e6;                            // ~6.0 TB/s
-constexpr double kBlockUsF64[4] = {35e-6, 42e-6, 48e-6, 56e-6};     // r = 1, 2, 4, 8
-constexpr double kBlockUsF32[4] = {50e-6, 58e-6, 66e-6, 78e-6};
+// B200 cost model of one SpMV through a converted handle's default kernel
+// choice (spc5_b200/tune_fit.py fits it from timings on a B200, 148 SMs at
+// 1.965 GHz): for value type, r and regime (0: the row kernel, every
+// block-row fits its staging buffers; 1: the length-sorted plan),
+//     t_us = t0 + nnz * (d0 + d1 / a + d2 / a^2),  a = nnz / blocks_r,
+// the time per value keyed by the average number of values per block, as the
+// reference's SPC5_find_best model is (src/spc5.hpp:1157-1212).
+// Value type (F64, F32, F32_V8) x r (1, 2, 4, 8) x regime: {t0, d0, d1, d2}.
+constexpr double kModel[3][4][2][4] = {
+    {
+        {{1.027079e+01, -2.714134e-07, 9.285081e-06, 1.994012e-06}, {1.027079e+01, 1.134102e-05, 0.000000e+00, 0.000000e+00}},
+        {{1.046586e+01, 6.170896e-07, 9.230068e-06, 9.138698e-06}, {1.046586e+01, 1.525453e-05, 0.000000e+00, 0.000000e+00}},
+        {{1.004610e+01, 1.547721e-06, 1.189384e-05, 2.402879e-05}, {1.004610e+01, 1.887387e-05, 0.000000e+00, 0.000000e+00}},
+        {{1.004540e+01, 6.250567e-07, 5.782892e-05, -8.901463e-05}, {1.004540e+01, 3.599312e-05, 0.000000e+00, 0.000000e+00}},
+    },
+    {
+        {{1.009044e+01, 2.953275e-07, 6.279096e-06, 1.099184e-05}, {1.009044e+01, 9.677628e-06, 0.000000e+00, 0.000000e+00}},
+        {{1.008880e+01, 1.137428e-06, 1.740009e-06, 3.621405e-05}, {1.008880e+01, 1.482245e-05, 0.000000e+00, 0.000000e+00}},
+        {{1.020511e+01, 1.170424e-06, 1.023505e-05, 1.026359e-04}, {1.020511e+01, 3.810895e-05, 0.000000e+00, 0.000000e+00}},
+        {{1.034971e+01, -4.723864e-07, 8.071517e-05, -1.176461e-04}, {1.034971e+01, 4.555848e-05, 0.000000e+00, 0.000000e+00}},
+    },
+    {
+        {{9.690487e+00, -8.483423e-07, 1.129287e-05, 5.480109e-06}, {9.690487e+00, 1.022678e-05, 0.000000e+00, 0.000000e+00}},
+        {{9.904177e+00, 1.562250e-07, 1.131417e-05, 1.759617e-05}, {9.904177e+00, 1.857101e-05, 0.000000e+00, 0.000000e+00}},
+        {{1.008765e+01, 1.592180e-07, 2.480687e-05, 2.707475e-05}, {1.008765e+01, 2.423231e-05, 0.000000e+00, 0.000000e+00}},
+        {{1.044845e+01, -1.152926e-06, 8.811726e-05, -7.893453e-05}, {1.044845e+01, 4.799635e-05, 0.000000e+00, 0.000000e+00}},
+    },
+};
 
 int r_index(int r) { return r == 1 ? 0 : (r == 2 ? 1 : (r == 4 ? 2 : 3)); }
 
-double model_us(const spc5cuda_mat* m, int r, long nblocks) {
-    const double t_mem = spmv_bytes(m, r, nblocks) / kHbmBytesPerUs;
-    const double per = m->value_type == SPC5CUDA_F64 ? kBlockUsF64[r_index(r)] : kBlockUsF32[r_index(r)];
-    const double t_issue = double(nblocks) * per;
-    return std::max(t_mem, t_issue);
+double model_us(const spc5cuda_mat* m, int r, long nblocks, int regime) {
+    if (m->nnz == 0 || nblocks == 0) return 0.0;
+    const double* c = kModel[m->value_type][r_index(r)][regime];
+    const double a = double(m->nnz) / double(nblocks);
+    const double per_value = std::max(c[1] + c[2] / a + c[3] / (a * a), 1e-7);
+    return c[0] + double(m->nnz) * per_value;
 }
 
-// Converts the CSR handle to r into temporary arrays and times the SpMV
-// kernel (1 warm-up, 3 timed launches); returns microseconds per SpMV.
-double measure_us(const spc5cuda_mat* m, int r, cudaStream_t s) {
+// 1 when some block-row of the CSR handle at rows-per-block r is too large for
+// the row kernel's buffers (the handle would then run the sorted plan): the
+// block counts are brptr (scanned), the value counts come from rowptr.
+int plan_regime(const spc5cuda_mat* m, int r, const int* brptr, cudaStream_t s) {
     const int nbr = div_up(m->nrows, r);
-    const int vs = vs_of(m->value_type);
-    const size_t vb = size_t(value_bytes_of(m->value_type));
-    DevBuf brptr(sizeof(int) * size_t(nbr + 1), s);
-    const long nb = count_blocks(m, r, brptr.as<int>(), s);
-    const size_t stride = 4 + size_t(r) * mask_bytes_of(m->value_type);
-    DevBuf headers(stride * size_t(nb) + 16, s);
-    DevBuf values(vb * size_t(m->nnz) + 16, s);
     DevBuf valptr(sizeof(int) * size_t(nbr + 1), s);
-    const int ngroups = spmv_groups(vs, r);
-    DevBuf gstart(sizeof(int) * size_t(ngroups + 1), s);
-    DevBuf x(vb * size_t(m->ncols) + 16, s);
-    const size_t yb = m->value_type == SPC5CUDA_F32_V8 ? 8 : vb;  // F32_V8: FP64 y
-    DevBuf y(yb * size_t(m->nrows) + 16, s);
-    launch_emit(vs, r, m->nrows, m->rowptr.as<int>(), m->colidx.as<int>(), m->values.p, int(vb),
-                brptr.as<int>(), headers.as<uint8_t>(), values.p, s);
     launch_valptr_from_csr(r, m->nrows, m->rowptr.as<int>(), valptr.as<int>(), s);
-    launch_partition(nbr, brptr.as<int>(), ngroups, gstart.as<int>(), s);
-    SPC5_CUDA(cudaMemsetAsync(x.p, 0, vb * size_t(m->ncols) + 16, s));
+    int max_blocks = 0, max_values = 0;
+    blockrow_max(nbr, brptr, valptr.as<int>(), &max_blocks, &max_values, s);
+    return rows_fit(m->value_type, r, max_blocks, max_values) ? 0 : 1;
+}
+
+// A trial run: a temporary handle holding a copy of the CSR matrix is
+// converted to r the usual way (its default kernel choice: the row kernel or
+// the length-sorted plan) and its SpMV is timed (1 warm-up, 3 timed calls);
+// returns microseconds per SpMV.
+double measure_us(const spc5cuda_mat* m, int r, cudaStream_t s) {
+    spc5cuda_mat* t = nullptr;
+    auto ok = [](spc5cuda_status st) {
+        if (st != SPC5CUDA_OK) throw Error(st, "autotune trial run");
+    };
+    ok(spc5cuda_mat_create_csr(&t, m->value_type, m->nrows, m->ncols, m->nnz, m->rowptr.as<int>(),
+                               m->colidx.as<int>(), m->values.p, 1, s));
+    std::unique_ptr<spc5cuda_mat, spc5cuda_status (*)(spc5cuda_mat*)> guard(t, spc5cuda_mat_destroy);
+    ok(spc5cuda_convert(t, r_to_format(r), s));
+    const size_t xb = size_t(value_bytes_of(m->value_type));
+    const size_t yb = m->value_type == SPC5CUDA_F32 ? 4 : 8;  // F32_V8: FP64 y
+    DevBuf x(xb * size_t(m->ncols) + 16, s), y(yb * size_t(m->nrows) + 16, s);
+    SPC5_CUDA(cudaMemsetAsync(x.p, 0, xb * size_t(m->ncols) + 16, s));
     SPC5_CUDA(cudaMemsetAsync(y.p, 0, yb * size_t(m->nrows) + 16, s));
-    BetaView v;
-    v.r = r;
-    v.nrows = m->nrows;
-    v.nbr = nbr;
-    v.brptr = brptr.as<int>();
-    v.headers = headers.as<uint8_t>();
-    v.values = values.p;
-    v.valptr = valptr.as<int>();
-    v.gstart = gstart.as<int>();
-    v.ngroups = ngroups;
     auto run = [&] {
-        if (m->value_type == SPC5CUDA_F64)
-            launch_spmv_f64(v, x.as<double>(), y.as<double>(), s);
-        else if (m->value_type == SPC5CUDA_F32_V8)
-            launch_spmv_mixed8(v, x.as<float>(), y.as<double>(), s);
+        if (m->value_type == SPC5CUDA_F32_V8)
+            ok(spc5cuda_spmv_mixed(t, x.as<float>(), y.as<double>(), s));
         else
-            launch_spmv_f32(v, x.as<float>(), y.as<float>(), s);
+            ok(spc5cuda_spmv(t, x.p, y.p, s));
     };
     cudaEvent_t e0, e1;
     SPC5_CUDA(cudaEventCreate(&e0));
@@ -154,9 +160,11 @@ spc5cuda_status spc5cuda_autotune(const spc5cuda_mat* m, int mode, spc5cuda_tune
             DevBuf tmp(sizeof(int) * size_t(div_up(m->nrows, r) + 1), s);
             const long nb = m->nrows > 0 ? count_blocks(m, r, tmp.as<int>(), s) : 0;
             out->blocks[f] = nb;
-            const double us = mode == SPC5CUDA_TUNE_MODEL
-                                  ? model_us(m, r, nb)
-                                  : (m->nrows > 0 ? measure_us(m, r, s) : 0.0);
+            double us = 0.0;
+            if (m->nrows > 0) {
+                us = mode == SPC5CUDA_TUNE_MODEL ? model_us(m, r, nb, plan_regime(m, r, tmp.as<int>(), s))
+                                                 : measure_us(m, r, s);
+            }
             out->est_us[f] = us;
             if (f == 0 || us < best_us) {
                 best_us = us;

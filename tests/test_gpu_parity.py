@@ -90,6 +90,29 @@ def test_dropin_entry_points(cuda, golden, tag, dt, r):
             assert y.cpu().numpy().tobytes() == golden[f"{n}/{tag}/r{r}/y"].tobytes(), (n, fn.__name__)
 
 
+@pytest.mark.parametrize("tag,dt", DTYPES)
+@pytest.mark.parametrize("r", [1, 2, 4, 8])
+def test_dropin_takes_either_kernel(cuda, tag, dt, r):
+    """The drop-in symbols pick the row kernel or the group kernel on the
+    device (a block-row of a dense 1500-column row does not fit the row
+    kernel's buffers; the stencil's do): both give the oracle's bits, over
+    three accumulating calls that reuse the library's scratch pool."""
+    f = oracle.beta_spmv_f64 if dt == np.float64 else oracle.beta_spmv_f32
+    for csr in (M.stencil27(14), M.dense(1500), M.powerlaw(30000, seed=13)):
+        vals = csr.values.astype(dt)
+        brptr, headers, ov = oracle.csr_to_beta(r, csr.rowptr, csr.colidx, vals)
+        x = M.x_vector(csr.ncols, 8, dt)
+        y0 = M.x_vector(csr.nrows, 9, dt)
+        yo = y0.copy()
+        args = (dev(brptr), dev(headers), dev(ov), dev(x))
+        y = dev(y0)
+        for _ in range(3):
+            f(r, csr.nrows, brptr, headers, ov, x, yo)
+            S.core_spmv_void(r, csr.nrows, *args, y)
+        torch.cuda.synchronize()
+        assert y.cpu().numpy().tobytes() == yo.tobytes(), csr.name
+
+
 @pytest.mark.parametrize("r", [1, 2, 4, 8])
 def test_handle_from_reference_arrays(cuda, golden, r):
     for n in names(golden)[:4]:
