@@ -634,6 +634,98 @@ def run_gpu(args):
 
 
 # ---------------------------------------------------------------------------
+# sharded: one matrix split across the ranks by block-row ranges, iterated
+# ---------------------------------------------------------------------------
+
+def run_sharded(args):
+    """--mode sharded: the power-law (or --workload) matrix cut into equal
+    block-row ranges, one per rank; a step is, for every format, one
+    iteration x <- A x: the NCCL all-gather of the x slices (in place, no
+    copy of x) and the local SpMV.  Strong scaling: the matrix is fixed."""
+    import torch
+    import torch.distributed as dist
+
+    from spc5_b200 import distributed as D
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    csr = build_workload(args.workload, args.size)
+    if csr.nrows != csr.ncols:
+        raise SystemExit("sharded iteration needs a square matrix")
+    shards, local_bytes = [], 0
+    for r in FORMATS:
+        sh = D.ShardedSpMV(csr, rank, world, r, dev, cuts="equal")
+        shards.append((r, sh))
+        nb = sh.mat.numberOfBlocks
+        local_bytes += spmv_bytes(sh.local.nnz, nb, r, sh.local.nrows, csr.ncols)
+    x0 = torch.from_numpy(M.x_vector(csr.ncols, 0)).to(dev)
+    xs = {r: x0[sh.r0:sh.r1].clone() for r, sh in shards}
+    stream = torch.cuda.current_stream()
+
+    def step(ev=None):
+        for i, (r, sh) in enumerate(shards):
+            if ev is not None:
+                ev[i][0].record(stream)
+            xf = sh.gather_x(xs[r])
+            if ev is not None:
+                ev[i][1].record(stream)
+            y = torch.zeros(sh.r1 - sh.r0, dtype=torch.float64, device=dev)
+            sh.local_spmv(xf, y)
+            # keep the iterate bounded: x <- A x / max|A x| would need a
+            # reduction; y is scaled by a constant instead (the bytes and the
+            # exchange are the same)
+            xs[r] = y.mul_(0.05)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev = [[[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in shards] for _ in range(args.steps)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        t0.record(stream)
+        for k in range(args.steps):
+            step(ev[k])
+        t1.record(stream)
+        clk.sample_now()
+        torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    gather_ms = sum(ev[k][i][0].elapsed_time(ev[k][i][1]) for k in range(args.steps) for i in range(len(shards)))
+    vals = torch.tensor([ms, gather_ms, float(local_bytes)], dtype=torch.float64, device=dev)
+    per_rank = [vals.clone() for _ in range(world)]
+    if world > 1:
+        dist.all_gather(per_rank, vals)
+    ms_max = max(float(v[0]) for v in per_rank)
+    total_bytes = sum(float(v[2]) for v in per_rank)
+    line = None
+    if rank == 0:
+        line = {"metric": METRIC + ", sharded iteration", "value": round(total_bytes * args.steps / (ms_max * 1e-3) / 1e9, 2),
+                "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": args.workload, "desc": workload_desc(args.workload, csr),
+                           "formats": list(FORMATS), "nrows": csr.nrows, "nnz": csr.nnz,
+                           "parallelism": f"block-row shards x{world}, NCCL all-gather of x per iteration"},
+                "per_rank": [{"rank": k, "gbs": round(float(v[2]) * args.steps / (float(v[0]) * 1e-3) / 1e9, 2),
+                              "allgather_us_per_step": round(float(v[1]) * 1e3 / args.steps, 1)}
+                             for k, v in enumerate(per_rank)],
+                "clocks": clk.summary(),
+                "gpu_launches": sum(sh.mat.spmv_launches for _, sh in shards) * args.steps}
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
 # batched workload: many banded matrices, per-matrix r, k right-hand sides
 # ---------------------------------------------------------------------------
 
@@ -866,6 +958,9 @@ def main():
     ap.add_argument("--formats", default="1,2,4,8", help="comma list of r to run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--mode", choices=["replicas", "sharded"], default="replicas",
+                    help="N > 1: every rank runs its own copy (replicas), or one matrix is cut into "
+                         "block-row shards iterated with an NCCL all-gather of x (sharded)")
     ap.add_argument("--no-extra", action="store_true",
                     help="default run: skip the stencil, Poisson and serving legs")
     ap.add_argument("--kernel", choices=["auto", "groups", "rows", "sorted"], default="auto",
@@ -883,6 +978,8 @@ def main():
         return run_batched(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.mode == "sharded":
+        return run_sharded(args)
     return run_gpu(args)
 
 

@@ -13,7 +13,11 @@ selects "nnz" or "blocks").
   its y slice; no collective on the data path.
 * iterative use (x_{t+1} = A x_t, square A): each rank holds only its x
   slice; ``iterate`` all-gathers the slices (one ``all_gather_into_tensor``
-  of ~N * 8 bytes over NVLink), then runs its local SpMV.
+  of ~N * 8 bytes over NVLink), then runs its local SpMV.  With equal-width
+  cuts (``cuts="equal"``: every rank but the last owns ``width`` rows, a
+  multiple of r) the gathered buffer is x itself: NCCL writes every slice in
+  place and the local SpMV reads a view of it, with no copy of x per
+  iteration.  Other cuts gather into a padded buffer and pack it once.
 """
 from __future__ import annotations
 
@@ -46,6 +50,14 @@ def partition_rows(rowptr, world: int, r: int = 1, weights=None):
     return np.asarray(cuts, dtype=np.int64)
 
 
+def equal_cuts(nrows: int, world: int, r: int = 1):
+    """Cuts of equal width (a multiple of r) for ``world`` ranks; the last
+    range is the remainder (possibly shorter or empty)."""
+    per = (nrows + world - 1) // world
+    width = ((per + r - 1) // r) * r
+    return np.asarray([min(nrows, k * width) for k in range(world)] + [nrows], dtype=np.int64)
+
+
 def row_slice(csr: CSR, r0: int, r1: int) -> CSR:
     """Rows [r0, r1) of a CSR matrix, all columns kept."""
     a, b = int(csr.rowptr[r0]), int(csr.rowptr[r1])
@@ -58,8 +70,22 @@ class ShardedSpMV:
 
     def __init__(self, csr: CSR, rank: int, world: int, r: int, device, dtype=np.float64,
                  cuts=None):
+        """``cuts``: None or "nnz" (nnz-balanced, block-row aligned), "equal"
+        (equal widths: the zero-copy gather of ``iterate``), or an array of
+        world + 1 row boundaries."""
         self.rank, self.world, self.r = rank, world, r
-        self.cuts = partition_rows(csr.rowptr, world, r) if cuts is None else np.asarray(cuts)
+        if cuts is None or (isinstance(cuts, str) and cuts == "nnz"):
+            self.cuts = partition_rows(csr.rowptr, world, r)
+        elif isinstance(cuts, str) and cuts == "equal":
+            self.cuts = equal_cuts(csr.nrows, world, r)
+        else:
+            self.cuts = np.asarray(cuts, dtype=np.int64)
+        counts = np.diff(self.cuts)
+        self.width = max(1, int(counts.max())) if len(counts) else 1
+        # the gathered buffer is x itself when rank k's slice starts at
+        # k * width (every slice but the trailing ones has the full width)
+        self.in_place = bool(all(int(self.cuts[k]) == min(csr.nrows, k * self.width) for k in range(world)))
+        self._xbuf = None
         self.r0, self.r1 = int(self.cuts[rank]), int(self.cuts[rank + 1])
         self.nrows, self.ncols = csr.nrows, csr.ncols
         self.local = row_slice(csr, self.r0, self.r1)
@@ -85,17 +111,26 @@ class ShardedSpMV:
         return y_local
 
     def gather_x(self, x_local, group=None):
-        """All-gather the ranks' x slices into the full x (one collective)."""
+        """All-gather the ranks' x slices into the full x (one collective).
+        With equal-width cuts the result is a view of the gather buffer (no
+        copy of x); otherwise the padded slices are packed once."""
         import torch
         import torch.distributed as dist
+        if self.world == 1:
+            return x_local
+        w = self.width
+        if self._xbuf is None or self._xbuf.dtype != x_local.dtype or self._xbuf.device != x_local.device:
+            self._xbuf = torch.empty(w * self.world, dtype=x_local.dtype, device=x_local.device)
+            self._xsend = torch.zeros(w, dtype=x_local.dtype, device=x_local.device)
+        send = x_local
+        if x_local.numel() != w:  # a shorter (last) slice: padded to the width
+            self._xsend[: x_local.numel()].copy_(x_local)
+            send = self._xsend
+        dist.all_gather_into_tensor(self._xbuf, send, group=group)
+        if self.in_place:
+            return self._xbuf[: self.ncols]
         counts = np.diff(self.cuts)
-        width = int(counts.max())
-        buf = torch.zeros(width, dtype=x_local.dtype, device=x_local.device)
-        buf[: x_local.numel()] = x_local
-        out = torch.empty(width * self.world, dtype=x_local.dtype, device=x_local.device)
-        dist.all_gather_into_tensor(out, buf, group=group)
-        parts = [out[k * width: k * width + int(counts[k])] for k in range(self.world)]
-        return torch.cat(parts)
+        return torch.cat([self._xbuf[k * w: k * w + int(counts[k])] for k in range(self.world)])
 
     def iterate(self, x_local, group=None):
         """x_next slice = A[r0:r1, :] x for a square A whose x is sharded like y."""

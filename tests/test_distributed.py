@@ -48,14 +48,28 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _worker(rank, world, port, r, out_path):
+def test_equal_cuts_properties():
+    for n in (1, 7, 1000, 6001):
+        for world in (1, 2, 3, 8):
+            for r in (1, 4, 8):
+                cuts = D.equal_cuts(n, world, r)
+                counts = np.diff(cuts)
+                assert cuts[0] == 0 and cuts[-1] == n and len(cuts) == world + 1
+                assert np.all(counts >= 0) and all(c % r == 0 or c == n for c in cuts)
+                width = counts.max()
+                assert all(cuts[k] == min(n, k * width) for k in range(world))
+
+
+def _worker(rank, world, port, r, out_path, cuts="nnz"):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         csr = M.powerlaw(6000, seed=11)
         x = torch.from_numpy(M.x_vector(csr.ncols, 3))
-        sh = OracleShard(csr, rank, world, r, device="cpu")
+        sh = OracleShard(csr, rank, world, r, device="cpu", cuts=cuts)
+        if cuts == "equal":
+            assert sh.in_place
         # one-shot, replicated x
         y_local = torch.zeros(sh.r1 - sh.r0, dtype=torch.float64)
         sh.spmv(x, y_local)
@@ -72,11 +86,14 @@ def _worker(rank, world, port, r, out_path):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("r", [1, 4])
-def test_two_ranks_match_single_matrix(r, tmp_path):
+@pytest.mark.parametrize("r,cuts", [(1, "nnz"), (4, "nnz"), (1, "equal"), (8, "equal")])
+def test_two_ranks_match_single_matrix(r, cuts, tmp_path):
+    """The real ShardedSpMV host path on two gloo ranks -- the block-row
+    aligned cuts, the x all-gather (in place for equal-width cuts, packed
+    otherwise) and iterate -- with the oracle as each rank's local SpMV."""
     out = str(tmp_path / "ranks.npz")
     port = _free_port()
-    mp.spawn(_worker, args=(2, port, r, out), nprocs=2, join=True)
+    mp.spawn(_worker, args=(2, port, r, out, cuts), nprocs=2, join=True)
     got = np.load(out)
     csr = M.powerlaw(6000, seed=11)
     x = M.x_vector(csr.ncols, 3)
