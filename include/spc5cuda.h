@@ -85,9 +85,13 @@ SPC5CUDA_API void spc5cuda_set_stream(void* stream);
  *   core_SPC5_8rVc_Spmv_{double,float}  spc5.hpp:895-902
  * y[0..nbRows) += A x.  The value offset of every block-row is not stored
  * in the format, so each call first derives it from the headers (one extra
- * pass over the header array, stream-ordered scratch of ceil(nbRows/r)+1
- * ints from cudaMallocAsync).  The handle API below keeps it resident.
- * Errors: spc5cuda_get_last_error().
+ * pass over the header array), tests on the device whether every block-row
+ * fits the row kernel's staging buffers, and runs the row kernel if so, else
+ * the group kernel (both enqueued, each gated on that device flag: no host
+ * round trip).  Scratch (block-row offsets and work splits) comes from a
+ * stream-ordered memory pool the library keeps per device.  The handle API
+ * below keeps the offsets resident and adds the length-sorted plan for
+ * irregular matrices.  Errors: spc5cuda_get_last_error().
  * ---------------------------------------------------------------------- */
 SPC5CUDA_API void core_SPC5_1rVc_Spmv_double(const long int nbRows, const int* rowsSizes,
                                 const unsigned char* blocksColumnIndexesWithMasks,
