@@ -817,7 +817,7 @@ def serve_pool():
             M.powerlaw(2_000_000, seed=24), M.stencil27(126)]
 
 
-def serve_leg(args, rates, seconds, precisions=(False, True)):
+def serve_leg(args, rates, seconds, precisions=(False, True), plan_serial=False):
     """The request loop over the 64-matrix pool at each offered rate (Poisson
     arrivals, Zipf(1.1) matrix choice) for each precision (False: FP64, True:
     mixed in the 8-column layout); one result dict per (precision, rate)."""
@@ -839,7 +839,7 @@ def serve_leg(args, rates, seconds, precisions=(False, True)):
                 # the SpMM on the handle's own arrays
                 S.CSR_to_SPC5(m, S.FORMAT_OF_R[1 if csr.name.startswith("powerlaw") else 4])
                 mats.append((m, csr))
-        srv = S.Server(slots=args.slots, max_k=16, mixed=mixed)
+        srv = S.Server(slots=args.slots, max_k=16, mixed=mixed, plan_serial=plan_serial)
         ids = [srv.add_matrix(m) for m, _ in mats]
         resident = srv.stats()["resident_bytes"]
         xs = [torch.from_numpy(M.x_vector(csr.ncols, 500 + i, dt)).cuda() for i, csr in enumerate(distinct)]
@@ -897,7 +897,7 @@ def run_serve(args):
     import torch
     torch.cuda.set_device(0)
     rates = [float(t) for t in args.rates.split(",")]
-    results = serve_leg(args, rates, args.serve_seconds)
+    results = serve_leg(args, rates, args.serve_seconds, plan_serial=args.plan_serial)
     best = max(r["req_per_s"] for r in results if r["precision"] == "f64")
     line = {"metric": "served SpMV req/s and p50/p99 latency", "value": best, "unit": "req/s",
             "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -953,6 +953,8 @@ def main():
     ap.add_argument("--rates", default="5000,20000,50000", help="serving arrival rates (req/s)")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--slots", type=int, default=4)
+    ap.add_argument("--plan-serial", action="store_true",
+                    help="serve: sorted-plan matrices run their parts in order on the slot's stream")
     ap.add_argument("--size", type=int, default=None,
                     help="smaller workload for profiling (rows for powerlaw, grid edge for stencil27)")
     ap.add_argument("--formats", default="1,2,4,8", help="comma list of r to run")

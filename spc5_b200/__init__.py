@@ -77,7 +77,7 @@ class spc5cuda_tune(C.Structure):
 
 class spc5cuda_server_config(C.Structure):
     _fields_ = [("slots", C.c_int), ("max_k", C.c_int), ("hbm_budget", C.c_long), ("mixed", C.c_int),
-                ("pad", C.c_int)]
+                ("plan_serial", C.c_int)]
 
 
 class spc5cuda_server_stats(C.Structure):
@@ -548,12 +548,13 @@ class Server:
     same-matrix requests into multi-RHS launches, admission by HBM footprint,
     latency percentiles).  A request computes y = A x for device tensors."""
 
-    def __init__(self, slots=4, max_k=16, hbm_budget=None, mixed=False):
+    def __init__(self, slots=4, max_k=16, hbm_budget=None, mixed=False, plan_serial=False):
         import torch
         if hbm_budget is None:
             free, _ = torch.cuda.mem_get_info()
             hbm_budget = int(free * 0.9)
-        cfg = spc5cuda_server_config(int(slots), int(max_k), int(hbm_budget), 1 if mixed else 0, 0)
+        cfg = spc5cuda_server_config(int(slots), int(max_k), int(hbm_budget), 1 if mixed else 0,
+                                     1 if plan_serial else 0)
         self.mixed = bool(mixed)
         self._h = C.c_void_p()
         self._mats = []

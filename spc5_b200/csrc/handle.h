@@ -163,13 +163,16 @@ struct SortedPlan {
 // and the view of one of its parts.
 void build_sorted_plan(spc5cuda_mat* m, cudaStream_t s);
 BetaView plan_view(const spc5cuda_mat* m, const SpmvPart& part);
-// y += A x through the plan (x, y of the handle's types; mixed: F32 handle,
-// float x, double y).
-void plan_spmv(const spc5cuda_mat* m, const void* x, void* y, bool mixed, cudaStream_t s);
+// y += A x through the plan (x, y of the handle's types; mixed: F32 or
+// F32_V8 handle, float x, double y).  fork: run the parts concurrently on the
+// plan's two streams and join them back to s (one such call at a time per
+// handle); otherwise one after another on s, so that calls on different
+// streams (the request loop's slots) overlap without sharing plan streams.
+void plan_spmv(const spc5cuda_mat* m, const void* x, void* y, bool mixed, cudaStream_t s, bool fork = true);
 // Y += A X through the plan with the staged SpMM (element (row i, rhs q) of
 // X at x[i * ldx + q * xcs], likewise Y).
 void plan_spmm(const spc5cuda_mat* m, int k, const void* x, long ldx, long xcs, void* y, long ldy, long ycs,
-               bool mixed, cudaStream_t s);
+               bool mixed, cudaStream_t s, bool fork = true);
 
 }  // namespace spc5cuda
 

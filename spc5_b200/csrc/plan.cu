@@ -403,8 +403,14 @@ namespace {
 // those on the caller's stream; all start after the work already queued on s
 // and s waits for all of them.
 template <class F>
-void run_parts(const spc5cuda_mat* m, cudaStream_t s, F&& launch) {
+void run_parts(const spc5cuda_mat* m, cudaStream_t s, bool fork, F&& launch) {
     SortedPlan& p = *m->plan;
+    if (!fork) {
+        // the parts one after another on the caller's stream: no shared plan
+        // streams, so calls on different streams overlap freely
+        for (const auto& part : p.parts) launch(plan_view(m, part), s);
+        return;
+    }
     std::lock_guard<std::mutex> lk(p.mu);
     SPC5_CUDA(cudaEventRecord(p.fork, s));
     for (auto st : p.aux) SPC5_CUDA(cudaStreamWaitEvent(st, p.fork, 0));
@@ -427,9 +433,9 @@ void run_parts(const spc5cuda_mat* m, cudaStream_t s, F&& launch) {
 
 }  // namespace
 
-void plan_spmv(const spc5cuda_mat* m, const void* x, void* y, bool mixed, cudaStream_t s) {
+void plan_spmv(const spc5cuda_mat* m, const void* x, void* y, bool mixed, cudaStream_t s, bool fork) {
     // the launchers pick the row kernel when the view has warp ranges
-    run_parts(m, s, [&](const BetaView& v, cudaStream_t st) {
+    run_parts(m, s, fork, [&](const BetaView& v, cudaStream_t st) {
         if (m->value_type == SPC5CUDA_F64)
             launch_spmv_f64(v, static_cast<const double*>(x), static_cast<double*>(y), st);
         else if (m->value_type == SPC5CUDA_F32_V8)
@@ -442,8 +448,8 @@ void plan_spmv(const spc5cuda_mat* m, const void* x, void* y, bool mixed, cudaSt
 }
 
 void plan_spmm(const spc5cuda_mat* m, int k, const void* x, long ldx, long xcs, void* y, long ldy, long ycs,
-               bool mixed, cudaStream_t s) {
-    run_parts(m, s, [&](const BetaView& v, cudaStream_t st) {
+               bool mixed, cudaStream_t s, bool fork) {
+    run_parts(m, s, fork, [&](const BetaView& v, cudaStream_t st) {
         if (!v.wstart) throw Error(SPC5CUDA_ERR_INVALID, "plan part without warp ranges");
         if (m->value_type == SPC5CUDA_F64)
             launch_spmm_rows_f64(v, k, static_cast<const double*>(x), ldx, xcs, static_cast<double*>(y), ldy, ycs,

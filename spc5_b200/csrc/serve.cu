@@ -154,7 +154,7 @@ bool spc5cuda_server::dispatch(Slot& sl) {
         void* y0 = io[0].second;
         SPC5_CUDA(cudaMemsetAsync(y0, 0, size_t(m->nrows) * yb, sl.stream));
         if (m->use_plan())
-            plan_spmv(m, io[0].first, y0, cfg.mixed, sl.stream);
+            plan_spmv(m, io[0].first, y0, cfg.mixed, sl.stream, cfg.plan_serial == 0);
         else if (cfg.mixed && m->value_type == SPC5CUDA_F32_V8)
             launch_spmv_mixed8(m->view(), static_cast<const float*>(io[0].first), static_cast<double*>(y0),
                                sl.stream);
@@ -173,7 +173,7 @@ bool spc5cuda_server::dispatch(Slot& sl) {
                                   cudaMemcpyDeviceToDevice, sl.stream));
     SPC5_CUDA(cudaMemsetAsync(Y, 0, size_t(k) * ldY * yb, sl.stream));
     if (m->use_plan())
-        plan_spmm(m, k, X, 1, ldX, Y, 1, ldY, cfg.mixed, sl.stream);
+        plan_spmm(m, k, X, 1, ldX, Y, 1, ldY, cfg.mixed, sl.stream, cfg.plan_serial == 0);
     else if (cfg.mixed && m->value_type == SPC5CUDA_F32_V8)
         launch_spmm_mixed8(m->spmm_view(), k, reinterpret_cast<const float*>(X), 1, ldX,
                            reinterpret_cast<double*>(Y), 1, ldY, sl.stream);
