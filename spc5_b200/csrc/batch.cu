@@ -65,6 +65,9 @@ spc5cuda_status spc5cuda_batch_create(spc5cuda_batch** out, int n, spc5cuda_mat*
                 require(mixed ? (m->value_type == SPC5CUDA_F32 || m->value_type == SPC5CUDA_F32_V8)
                               : m->value_type != SPC5CUDA_F32_V8,
                         SPC5CUDA_ERR_FORMAT, "mixed batches need F32 or F32_V8 matrices, the others F64 or F32");
+                // batch graphs read the reference order: a handle whose
+                // sorted copy held the only one keeps both from here on
+                const_cast<spc5cuda_mat*>(m)->restore_original(s);
                 BatchMat& b = hm[size_t(i)];
                 b.brptr = m->brptr.as<int>();
                 b.headers = m->headers.as<uint8_t>();

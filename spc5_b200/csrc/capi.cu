@@ -343,9 +343,12 @@ spc5cuda_status spc5cuda_mat_set_kernel(spc5cuda_mat* m, int kernel) {
             require(m->rows_ok, SPC5CUDA_ERR_UNSUPPORTED, "a block-row exceeds the row kernel's buffers");
         m->kernel = kernel;
         if (m->r != 0 && m->wants_plan() && !m->plan) build_sorted_plan(m, nullptr);
-        // the group and row kernels run on the handle's own arrays: release the copy
-        if (kernel == SPC5CUDA_KERNEL_GROUPS || kernel == SPC5CUDA_KERNEL_ROWS) {
-            if (m->plan) SPC5_CUDA(cudaDeviceSynchronize());  // no SpMV may still read it
+        // the group and row kernels run on the handle's own arrays: bring
+        // them back from the sorted copy if it held the only one, then
+        // release the copy
+        if (m->plan && !m->use_plan()) {
+            m->restore_original(nullptr);
+            SPC5_CUDA(cudaDeviceSynchronize());  // no SpMV may still read the copy
             m->plan.reset();
         }
     });
@@ -430,10 +433,21 @@ spc5cuda_status spc5cuda_get_arrays(const spc5cuda_mat* m, int* rowsSize, unsign
         const cudaMemcpyKind kind = to_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
         if (rowsSize)
             SPC5_CUDA(cudaMemcpyAsync(rowsSize, m->brptr.p, m->brptr.bytes, kind, s));
-        if (headers && m->headers.bytes)
-            SPC5_CUDA(cudaMemcpyAsync(headers, m->headers.p, m->headers.bytes, kind, s));
-        if (values && m->values.bytes)
-            SPC5_CUDA(cudaMemcpyAsync(values, m->values.p, m->values.bytes, kind, s));
+        const void* hsrc = m->headers.p;
+        const void* vsrc = m->values.p;
+        // the sorted copy holds the only one: the reference order, rebuilt
+        const bool rebuild = m->original_dropped && (headers || values);
+        DevBuf th(rebuild ? std::max<size_t>(16, m->header_bytes()) : 0, s);
+        DevBuf tv(rebuild ? std::max<size_t>(16, m->value_bytes()) : 0, s);
+        if (rebuild) {
+            rebuild_original(m, th.as<uint8_t>(), tv.p, s);
+            hsrc = th.p;
+            vsrc = tv.p;
+        }
+        if (headers && m->header_bytes())
+            SPC5_CUDA(cudaMemcpyAsync(headers, hsrc, m->header_bytes(), kind, s));
+        if (values && m->value_bytes())
+            SPC5_CUDA(cudaMemcpyAsync(values, vsrc, m->value_bytes(), kind, s));
         if (to_host) SPC5_CUDA(cudaStreamSynchronize(s));
     });
 }

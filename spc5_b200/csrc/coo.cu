@@ -104,15 +104,23 @@ spc5cuda_status spc5cuda_decode_coo(const spc5cuda_mat* m, int* rows, int* cols,
         require(rows && cols && values, SPC5CUDA_ERR_INVALID, "null output");
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         const int nbr = m->nbr();
+        const uint8_t* hdr = m->headers.as<uint8_t>();
+        const void* vals = m->values.p;
+        const bool rebuild = m->original_dropped;  // the sorted copy holds the only one
+        DevBuf th(rebuild ? std::max<size_t>(16, m->header_bytes()) : 0, s);
+        DevBuf tv(rebuild ? std::max<size_t>(16, m->value_bytes()) : 0, s);
+        if (rebuild) {
+            rebuild_original(m, th.as<uint8_t>(), tv.p, s);
+            hdr = th.as<uint8_t>();
+            vals = tv.p;
+        }
         if (mask_bytes_of(m->value_type) == 1)
-            k_decode<1><<<grid_for(nbr), 256, 0, s>>>(m->r, m->nrows, nbr, m->brptr.as<int>(),
-                                                      m->headers.as<uint8_t>(), m->valptr.as<int>(),
-                                                      m->values.p, value_bytes_of(m->value_type),
+            k_decode<1><<<grid_for(nbr), 256, 0, s>>>(m->r, m->nrows, nbr, m->brptr.as<int>(), hdr,
+                                                      m->valptr.as<int>(), vals, value_bytes_of(m->value_type),
                                                       rows, cols, values);
         else
-            k_decode<2><<<grid_for(nbr), 256, 0, s>>>(m->r, m->nrows, nbr, m->brptr.as<int>(),
-                                                      m->headers.as<uint8_t>(), m->valptr.as<int>(),
-                                                      m->values.p, value_bytes_of(m->value_type),
+            k_decode<2><<<grid_for(nbr), 256, 0, s>>>(m->r, m->nrows, nbr, m->brptr.as<int>(), hdr,
+                                                      m->valptr.as<int>(), vals, value_bytes_of(m->value_type),
                                                       rows, cols, values);
         SPC5_CUDA(cudaGetLastError());
     });

@@ -163,6 +163,9 @@ struct SortedPlan {
 // and the view of one of its parts.
 void build_sorted_plan(spc5cuda_mat* m, cudaStream_t s);
 BetaView plan_view(const spc5cuda_mat* m, const SpmvPart& part);
+// The reference-order headers and values of a handle whose plan holds the
+// only copy, written to device buffers of m->headers / m->values size.
+void rebuild_original(const spc5cuda_mat* m, uint8_t* headers, void* values, cudaStream_t s);
 // y += A x through the plan (x, y of the handle's types; mixed: F32 or
 // F32_V8 handle, float x, double y).  fork: run the parts concurrently on the
 // plan's two streams and join them back to s (one such call at a time per
@@ -199,6 +202,9 @@ struct spc5cuda_mat {
     int kernel = SPC5CUDA_KERNEL_AUTO;  // SpMV kernel choice (spc5cuda_mat_set_kernel)
     bool rows_ok = false;               // every block-row fits the row kernel's buffers
     std::unique_ptr<spc5cuda::SortedPlan> plan;  // length-sorted copy (irregular matrices)
+    // the plan holds the only copy of headers and values (set when the plan
+    // is built and serves SpMV): the reference order is rebuilt on demand
+    bool original_dropped = false;
 
     int nbr() const { return r ? spc5cuda::div_up(nrows, r) : 0; }
     BetaView view() const {
@@ -247,6 +253,23 @@ struct spc5cuda_mat {
     bool wants_plan() const {
         return kernel == SPC5CUDA_KERNEL_SORTED || (kernel == SPC5CUDA_KERNEL_AUTO && !rows_ok);
     }
+    size_t header_bytes() const {
+        return size_t(nblocks) * size_t(4 + r * spc5cuda::mask_bytes_of(value_type));
+    }
+    size_t value_bytes() const { return size_t(nnz) * size_t(spc5cuda::value_bytes_of(value_type)); }
+    // Bring the reference-order headers and values back into the handle
+    // (synchronises s); a no-op unless the plan holds the only copy.
+    void restore_original(cudaStream_t s) {
+        if (!original_dropped) return;
+        Owned h, v;
+        h.alloc(std::max<size_t>(header_bytes(), 16));
+        v.alloc(std::max<size_t>(value_bytes(), 16));
+        spc5cuda::rebuild_original(this, h.as<uint8_t>(), v.p, s);
+        SPC5_CUDA(cudaStreamSynchronize(s));
+        headers = std::move(h);
+        values = std::move(v);
+        original_dropped = false;
+    }
     long device_bytes() const {
         return long(rowptr.bytes + colidx.bytes + values.bytes + brptr.bytes + headers.bytes +
                     valptr.bytes + gstart.bytes + wstart.bytes) + (plan ? plan->bytes() : 0L);
@@ -270,6 +293,7 @@ struct spc5cuda_mat {
             nwarps = 0;
             wstart.release();
         }
+        restore_original(s);  // the plan may hold the only copy
         plan.reset();
         if (wants_plan()) spc5cuda::build_sorted_plan(this, s);
     }

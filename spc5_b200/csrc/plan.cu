@@ -49,6 +49,57 @@ __global__ void k_sorted_counts(int nbr, const int* __restrict__ perm, const int
     }
 }
 
+// The reference order back from the sorted copy, sorted block-rows
+// [a, nbr): sorted block-row i goes to block-row perm[i]'s offsets (one warp
+// per block-row).
+template <class V>
+__global__ void k_unsorted_copy(int a, int nbr, const int* __restrict__ perm, const int* __restrict__ sbrptr,
+                                const int* __restrict__ svalptr, const int* __restrict__ brptr,
+                                const int* __restrict__ valptr, int stride, const uint8_t* __restrict__ shdr,
+                                uint8_t* __restrict__ hdr, const V* __restrict__ svals, V* __restrict__ vals) {
+    const int lane = threadIdx.x & 31;
+    const long warps = long(gridDim.x) * blockDim.x / 32;
+    for (long i = a + (long(blockIdx.x) * blockDim.x + threadIdx.x) / 32; i < nbr; i += warps) {
+        const int p = perm[i];
+        const long h0 = long(sbrptr[i]) * stride, hn = long(sbrptr[i + 1]) * stride - h0;
+        const long d0 = long(brptr[p]) * stride;
+        for (long k = lane; k < hn; k += 32) hdr[d0 + k] = shdr[h0 + k];
+        const long v0 = svalptr[i], vn = long(svalptr[i + 1]) - v0;
+        const long w0 = valptr[p];
+        for (long k = lane; k < vn; k += 32) vals[w0 + k] = svals[v0 + k];
+    }
+}
+
+// The same for the segmented block-rows [0, nlong): block-row i is warp
+// g = i / spw, slot s = i % spw of the segment layout; its segment k is
+// segment row split[g] + k n_g + s (n_g = its warp's block-rows), and its
+// segments, in order, are its blocks and values in order.
+template <class V>
+__global__ void k_unsegmented_copy(int nlong, int spw, const int* __restrict__ perm, const int* __restrict__ split,
+                                   const int* __restrict__ vbrptr, const int* __restrict__ vvalptr,
+                                   const int* __restrict__ brptr, const int* __restrict__ valptr, int stride,
+                                   const uint8_t* __restrict__ shdr, uint8_t* __restrict__ hdr,
+                                   const V* __restrict__ svals, V* __restrict__ vals) {
+    const int lane = threadIdx.x & 31;
+    const long warps = long(gridDim.x) * blockDim.x / 32;
+    for (long i = (long(blockIdx.x) * blockDim.x + threadIdx.x) / 32; i < nlong; i += warps) {
+        const int g = int(i) / spw, s = int(i) % spw;
+        const int n = min(spw, nlong - g * spw);
+        const int rows = split[g + 1] - split[g];
+        const int p = perm[i];
+        long hb = long(brptr[p]) * stride, vb = valptr[p];
+        for (int k = 0; k * n < rows; ++k) {
+            const int j = split[g] + k * n + s;
+            const long h0 = long(vbrptr[j]) * stride, hn = long(vbrptr[j + 1]) * stride - h0;
+            for (long t = lane; t < hn; t += 32) hdr[hb + t] = shdr[h0 + t];
+            hb += hn;
+            const long v0 = vvalptr[j], vn = long(vvalptr[j + 1]) - v0;
+            for (long t = lane; t < vn; t += 32) vals[vb + t] = svals[v0 + t];
+            vb += vn;
+        }
+    }
+}
+
 // Copy block-row perm[i] to sorted position i: one warp per block-row.
 template <class V>
 __global__ void k_sorted_copy(int nbr, const int* __restrict__ perm, const int* __restrict__ brptr,
@@ -366,6 +417,54 @@ void build_sorted_plan(spc5cuda_mat* m, cudaStream_t s) {
     for (auto& e : plan->join) SPC5_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     SPC5_CUDA(cudaStreamSynchronize(s));
     m->plan = std::move(plan);
+    // the sorted copy serves every SpMV now: the reference-order headers and
+    // values are rebuilt from it when a call needs them (restore_original)
+    if (m->use_plan()) {
+        m->headers.release();
+        m->values.release();
+        m->original_dropped = true;
+    }
+}
+
+void rebuild_original(const spc5cuda_mat* m, uint8_t* headers, void* values, cudaStream_t s) {
+    const SortedPlan& p = *m->plan;
+    const int nbr = m->nbr();
+    const int stride = 4 + m->r * mask_bytes_of(m->value_type);
+    const bool f64 = m->value_type == SPC5CUDA_F64;
+    const int threads = 256;
+    const SpmvPart* seg = nullptr;
+    for (const auto& part : p.parts)
+        if (part.nseg > 0) seg = &part;
+    const int nlong = seg ? seg->nseg : 0;
+    if (nbr > nlong) {
+        const int blocks = std::max(1, std::min(div_up(long(nbr - nlong) * 32, threads), sm_count() * 16));
+        if (f64)
+            k_unsorted_copy<double><<<blocks, threads, 0, s>>>(
+                nlong, nbr, p.perm.as<int>(), p.sbrptr.as<int>(), p.svalptr.as<int>(), m->brptr.as<int>(),
+                m->valptr.as<int>(), stride, p.sheaders.as<uint8_t>(), headers, p.svalues.as<double>(),
+                static_cast<double*>(values));
+        else
+            k_unsorted_copy<float><<<blocks, threads, 0, s>>>(
+                nlong, nbr, p.perm.as<int>(), p.sbrptr.as<int>(), p.svalptr.as<int>(), m->brptr.as<int>(),
+                m->valptr.as<int>(), stride, p.sheaders.as<uint8_t>(), headers, p.svalues.as<float>(),
+                static_cast<float*>(values));
+        SPC5_CUDA(cudaGetLastError());
+    }
+    if (nlong > 0) {
+        const int spw = 32 / seg->lanes;
+        const int blocks = std::max(1, std::min(div_up(long(nlong) * 32, threads), sm_count() * 16));
+        if (f64)
+            k_unsegmented_copy<double><<<blocks, threads, 0, s>>>(
+                nlong, spw, p.perm.as<int>(), seg->split.as<int>(), seg->vbrptr.as<int>(), seg->vvalptr.as<int>(),
+                m->brptr.as<int>(), m->valptr.as<int>(), stride, p.sheaders.as<uint8_t>(), headers,
+                p.svalues.as<double>(), static_cast<double*>(values));
+        else
+            k_unsegmented_copy<float><<<blocks, threads, 0, s>>>(
+                nlong, spw, p.perm.as<int>(), seg->split.as<int>(), seg->vbrptr.as<int>(), seg->vvalptr.as<int>(),
+                m->brptr.as<int>(), m->valptr.as<int>(), stride, p.sheaders.as<uint8_t>(), headers,
+                p.svalues.as<float>(), static_cast<float*>(values));
+        SPC5_CUDA(cudaGetLastError());
+    }
 }
 
 BetaView plan_view(const spc5cuda_mat* m, const SpmvPart& part) {

@@ -237,10 +237,79 @@ def test_kernel_selection(cuda):
     assert pl.kernel == S.KERNEL_SORTED
     assert st.spmv_launches == 1 and pl.spmv_launches >= 2  # one launch per part of the plan
     before = pl.info().device_bytes
-    pl.set_kernel(S.KERNEL_GROUPS)  # releases the sorted copy
-    assert pl.kernel == S.KERNEL_GROUPS and pl.info().device_bytes < before
-    pl.set_kernel(S.KERNEL_AUTO)  # builds it again
+    pl.set_kernel(S.KERNEL_GROUPS)  # the reference order back, the sorted copy released
+    assert pl.kernel == S.KERNEL_GROUPS
+    pl.set_kernel(S.KERNEL_AUTO)  # builds it again, in place
     assert pl.kernel == S.KERNEL_SORTED and pl.info().device_bytes == before
+
+
+@pytest.mark.parametrize("vt", [S.F64, S.F32, S.F32_V8])
+@pytest.mark.parametrize("r", [1, 2, 4, 8])
+def test_sorted_plan_in_place(cuda, vt, r):
+    """A handle served by the length-sorted plan keeps one copy of its
+    headers and values (the sorted one): its device footprint is the beta
+    arrays plus int32 offsets.  The reference order rebuilt from that copy
+    (arrays(), decode_coo, a batch graph, the group kernel after set_kernel)
+    is the oracle's conversion, byte for byte, and every path's SpMV is the
+    oracle's."""
+    dt = np.float64 if vt == S.F64 else np.float32
+    mixed = vt == S.F32_V8
+    for csr in (M.powerlaw(60_000, seed=21), M.dense(4096)):  # the dense rows run in segments
+        m = S.csr_matrix(csr.rowptr, csr.colidx, csr.values.astype(dt), csr.ncols,
+                         value_type=S.F32_V8 if mixed else None)
+        m.set_kernel(S.KERNEL_SORTED)
+        S.CSR_to_SPC5(m, S.FORMAT_OF_R[r])
+        assert m.kernel == S.KERNEL_SORTED
+        inf = m.info()
+        nbr = (csr.nrows + r - 1) // r
+        vbytes = 8 if vt == S.F64 else 4
+        # headers + values once, int32 offsets (brptr, valptr, perm, sorted
+        # offsets, partitions) and the segments' offsets (a few % of the
+        # beta arrays for a matrix of long rows cut into many segments)
+        beta = inf.header_bytes + csr.nnz * vbytes
+        assert inf.device_bytes <= 1.05 * beta + 7 * 4 * (nbr + 1) + (1 << 20), \
+            (csr.name, inf.device_bytes, inf.header_bytes, csr.nnz)
+        conv = oracle.csr_to_beta_v8 if mixed else oracle.csr_to_beta
+        ob, oh, ov = conv(r, csr.rowptr, csr.colidx, csr.values.astype(dt))
+        gb, gh, gv = m.arrays()
+        assert np.array_equal(gb, ob) and np.array_equal(gh, oh) and gv.tobytes() == ov.tobytes(), csr.name
+        rows, cols, vals = (t.cpu().numpy() for t in S.decode_coo(m))
+        if not mixed:
+            orow, ocol, oval = oracle.beta_to_coo(r, csr.nrows, ob, oh, ov)
+            assert np.array_equal(rows, orow) and np.array_equal(cols, ocol) and vals.tobytes() == oval.tobytes()
+        order = np.lexsort((cols, rows))
+        assert np.array_equal(cols[order], csr.colidx)
+        assert vals[order].tobytes() == csr.values.astype(dt).tobytes()
+        assert inf.device_bytes == m.info().device_bytes  # nothing kept by the rebuilds
+        x = M.x_vector(csr.ncols, 5, dt)
+        y0 = M.x_vector(csr.nrows, 6, np.float64 if mixed else dt)
+        if mixed:
+            yo = oracle.beta_spmv_mixed8(r, csr.nrows, ob, oh, ov, x, y0.copy())
+        else:
+            yo = oracle_spmv(dt, r, csr.nrows, ob, oh, ov, x, y0.copy())
+        f = S.SPC5_Spmv_mixed if mixed else S.SPC5_Spmv
+        y = dev(y0)
+        f(m, dev(x), y)
+        torch.cuda.synchronize()
+        assert y.cpu().numpy().tobytes() == yo.tobytes(), (csr.name, "plan")
+        m.set_kernel(S.KERNEL_GROUPS)  # runs on the rebuilt reference order
+        y = dev(y0)
+        f(m, dev(x), y)
+        torch.cuda.synchronize()
+        assert y.cpu().numpy().tobytes() == yo.tobytes(), (csr.name, "groups")
+        m.set_kernel(S.KERNEL_SORTED)
+        assert m.kernel == S.KERNEL_SORTED and m.info().device_bytes == inf.device_bytes
+        # a batch graph reads the reference order: the handle keeps both copies
+        Y = dev(y0[:, None].copy())
+        b = S.Batch([m], [dev(x[:, None].copy())], [Y], mixed=mixed)
+        b.launch()
+        torch.cuda.synchronize()
+        assert Y.cpu().numpy()[:, 0].tobytes() == yo.tobytes(), (csr.name, "batch")
+        assert m.info().device_bytes > inf.device_bytes
+        y = dev(y0)
+        f(m, dev(x), y)
+        torch.cuda.synchronize()
+        assert y.cpu().numpy().tobytes() == yo.tobytes(), (csr.name, "plan after batch")
 
 
 @pytest.mark.parametrize("r", [1, 2, 4, 8])
