@@ -468,6 +468,9 @@ def spmv_leg(csr, args, dev, world, barrier, max_over_ranks, steps, warmup, e2e=
     peak, peak_kind = load_peaks()
     out = {"value": value, "ms": ms, "step_bytes": step_bytes, "mats": mats, "x": x, "y": y,
            "blocks": {r: m.numberOfBlocks for r, m in mats}, "flush": flush is not None,
+           "memory": {"device_gb": {str(r): round(m.info().device_bytes / 1e9, 3) for r, m in mats},
+                      "beta_gb": {str(r): round((m.info().header_bytes + csr.nnz * 8) / 1e9, 3) for r, m in mats},
+                      "note": "handle footprint on the device against its beta(r,8) headers and values"},
            "per_format_gbs": {str(r): round(bytes_of[r] / (per_r_ms[r] * 1e-3) / 1e9, 2) for r in FORMATS},
            "per_r_ms": per_r_ms, "bytes_of": bytes_of, "achieved": achieved, "peak": peak,
            "peak_kind": peak_kind, "clocks": clocks, "warm": warm,
@@ -584,6 +587,7 @@ def run_gpu(args):
                          "peak_kind": main["peak_kind"], "traffic": traffic, "traffic_source": traffic_src,
                          "kernel": ", ".join(sorted({KERNEL_NAME[m.kernel] for _, m in mats}))},
             "kernels": {str(r): KERNEL_NAME[m.kernel] for r, m in mats},
+            "memory": main["memory"],
             "e2e": main["e2e"],
             "gpu_launches": sum(m.spmv_launches for _, m in mats) * args.steps,
             "clocks": main["clocks"],
@@ -810,10 +814,11 @@ def run_batched(args):
 
 def serve_pool():
     """Eight distinct matrices (power-law and 27-point stencil styles, N from
-    ~50K to ~2M); each is registered eight times, giving 64 resident
-    matrices."""
-    return [M.powerlaw(50_000, seed=21), M.stencil27(60), M.powerlaw(300_000, seed=22),
-            M.stencil27(80), M.powerlaw(1_000_000, seed=23), M.stencil27(100),
+    50K to 2M, smallest first: the Zipf choice favours the small ones); each
+    is registered eight times, giving 64 resident matrices of about 20 GB in
+    FP64."""
+    return [M.powerlaw(50_000, seed=21), M.stencil27(100), M.powerlaw(1_500_000, seed=22),
+            M.stencil27(110), M.powerlaw(2_000_000, seed=23), M.stencil27(120),
             M.powerlaw(2_000_000, seed=24), M.stencil27(126)]
 
 
@@ -834,9 +839,10 @@ def serve_leg(args, rates, seconds, precisions=(False, True), plan_serial=False)
             for csr in distinct:
                 m = S.csr_matrix(csr.rowptr, csr.colidx, csr.values.astype(dt), csr.ncols,
                                  value_type=S.F32_V8 if mixed else None)
-                # default kernel choice: lone requests run the handle's SpMV
-                # (the length-sorted copy for the power-law matrices), batches
-                # the SpMM on the handle's own arrays
+                # default kernel choice: the length-sorted plan for the
+                # power-law matrices (its single copy of the arrays serves
+                # lone requests and batches alike), the row kernels for the
+                # stencils
                 S.CSR_to_SPC5(m, S.FORMAT_OF_R[1 if csr.name.startswith("powerlaw") else 4])
                 mats.append((m, csr))
         srv = S.Server(slots=args.slots, max_k=16, mixed=mixed, plan_serial=plan_serial)
@@ -924,7 +930,7 @@ TRAFFIC_RATIO = {"powerlaw": {1: 1.194, 2: 1.120, 4: 1.065, 8: 1.019},
 
 # spc5cuda_mat_kernel codes: SPC5CUDA_KERNEL_GROUPS = 1, SPC5CUDA_KERNEL_ROWS = 2
 KERNEL_NAME = {1: "k_spmv (group per block-row stream)", 2: "k_rows (thread per sub-row)",
-               3: "sorted plan (k_rows by block-row size; largest block-rows in segments)", 0: "unconverted"}
+               3: "sorted plan (k_rows by block-row size; largest block-rows as multiply-add chains, k_chain_spmv)", 0: "unconverted"}
 
 
 def select_kernel(m, which):

@@ -76,13 +76,12 @@ void spc5cuda::valptr_from_headers(int mask_bytes, int r, int nbr, const int* br
     exclusive_scan_i32(valptr, valptr, nbr, tmp.as<int>(), s);
 }
 
-namespace {
-
 // The library's own stream-ordered memory pool on the current device: the
-// per-call scratch of the drop-in symbols comes from it, and it keeps freed
-// memory for the next call (release threshold: never), so repeated calls do
-// not go back to the driver.  One pool per device for the process lifetime.
-cudaMemPool_t scratch_pool() {
+// per-call scratch of the drop-in symbols and of the plan's chain part comes
+// from it, and it keeps freed memory for the next call (release threshold:
+// never), so repeated calls do not go back to the driver.  One pool per
+// device for the process lifetime.
+cudaMemPool_t spc5cuda::scratch_pool() {
     static std::mutex mu;
     static cudaMemPool_t pools[64] = {};
     int dev = 0;
@@ -102,21 +101,7 @@ cudaMemPool_t scratch_pool() {
     return pools[dev];
 }
 
-// Stream-ordered scratch from scratch_pool().
-struct PoolBuf {
-    void* p = nullptr;
-    cudaStream_t s;
-    PoolBuf(size_t n, cudaStream_t st) : s(st) {
-        SPC5_CUDA(cudaMallocFromPoolAsync(&p, std::max<size_t>(n, 16), scratch_pool(), st));
-    }
-    ~PoolBuf() {
-        if (p) cudaFreeAsync(p, s);
-    }
-    PoolBuf(const PoolBuf&) = delete;
-    PoolBuf& operator=(const PoolBuf&) = delete;
-    template <class U>
-    U* as() const { return static_cast<U*>(p); }
-};
+namespace {
 
 // core_SPC5_{r}rVc_Spmv_{double,float} over device arrays without a handle.
 // Per call, all on the stream and without a host round trip: the value
@@ -359,7 +344,10 @@ spc5cuda_status spc5cuda_mat_spmv_launches(const spc5cuda_mat* m, int* launches)
         require(m && launches, SPC5CUDA_ERR_INVALID, "null");
         require(m->r != 0, SPC5CUDA_ERR_FORMAT, "matrix is not converted");
         if (m->nrows == 0) *launches = 0;
-        else if (m->use_plan()) *launches = int(m->plan->parts.size());
+        else if (m->use_plan()) {
+            *launches = 0;
+            for (const auto& part : m->plan->parts) *launches += part.chains ? 2 : 1;
+        }
         else *launches = 1;
     });
 }

@@ -32,6 +32,24 @@ struct DevBuf {
     T* as() const { return static_cast<T*>(p); }
 };
 
+// The library's stream-ordered memory pool on the current device (capi.cu),
+// and per-call scratch from it.
+cudaMemPool_t scratch_pool();
+struct PoolBuf {
+    void* p = nullptr;
+    cudaStream_t s;
+    PoolBuf(size_t n, cudaStream_t st) : s(st) {
+        SPC5_CUDA(cudaMallocFromPoolAsync(&p, n < 16 ? size_t(16) : n, scratch_pool(), st));
+    }
+    ~PoolBuf() {
+        if (p) cudaFreeAsync(p, s);
+    }
+    PoolBuf(const PoolBuf&) = delete;
+    PoolBuf& operator=(const PoolBuf&) = delete;
+    template <class U>
+    U* as() const { return static_cast<U*>(p); }
+};
+
 // Persistent device buffer owned by a matrix handle.
 struct Owned {
     void* p = nullptr;
@@ -120,17 +138,29 @@ inline void require(bool cond, spc5cuda_status s, const char* what) {
 // One part of the length-sorted plan: sorted block-rows [a, b), run by the
 // row kernel with `lanes` lanes per block-row (split: one range per warp), or
 // by the group kernel when lanes == 0 (split: one range per group); split
-// holds nsplit + 1 block-row starts.  A segmented part (nseg = b - a > 0,
-// a = 0) holds block-rows too large to stage: cut into segments that are,
-// interleaved per warp; vbrptr / vvalptr are the segments' block and value
-// offsets and split their per-warp ranges.
+// holds nsplit + 1 block-row starts.  The part of the block-rows too large
+// to stage (nseg = b - a > 0, a = 0) is either the chain part (chains: the
+// multiply-add chains below; two launches) or segmented: cut into segments
+// that are, interleaved per warp; vbrptr / vvalptr are the segments' block
+// and value offsets and split their per-warp ranges.
 struct SpmvPart {
     int lanes = 0;
     int a = 0, b = 0;
     int nseg = 0;
+    bool chains = false;
     Owned split;
     int nsplit = 0;
     Owned vbrptr, vvalptr;
+    // the chain part (chain.cu): one multiply-add chain per (block-row,
+    // sub-row, column) of the nseg largest block-rows, chain id
+    // (i * r + s) * VS + c.  The nchains non-empty ones, sorted by length
+    // (slen, corder: chain ids), cut into slices of 32 chains, entry j of the
+    // slice's lane l at slice_off[slice] + 32 j + l (cval: value, ccol: x
+    // index); cmask[i * r + s] bit c: chain c of that sub-row is not empty.
+    long nchains = 0;
+    long entries = 0;  // values in the chains
+    int nslices = 0;
+    Owned slen, corder, slice_off, cval, ccol, cmask;
 };
 
 // A copy of the matrix with its block-rows sorted by size (plan.cu).  Its
@@ -154,7 +184,9 @@ struct SortedPlan {
     }
     long bytes() const {
         long n = long(sbrptr.bytes + sheaders.bytes + svalues.bytes + svalptr.bytes + perm.bytes);
-        for (const auto& p : parts) n += long(p.split.bytes + p.vbrptr.bytes + p.vvalptr.bytes);
+        for (const auto& p : parts)
+            n += long(p.split.bytes + p.vbrptr.bytes + p.vvalptr.bytes + p.slen.bytes + p.corder.bytes +
+                      p.slice_off.bytes + p.cval.bytes + p.ccol.bytes + p.cmask.bytes);
         return n;
     }
 };
@@ -166,6 +198,16 @@ BetaView plan_view(const spc5cuda_mat* m, const SpmvPart& part);
 // The reference-order headers and values of a handle whose plan holds the
 // only copy, written to device buffers of m->headers / m->values size.
 void rebuild_original(const spc5cuda_mat* m, uint8_t* headers, void* values, cudaStream_t s);
+// The chain part (chain.cu): built from the sorted copy's block-rows
+// [0, part.nseg), whose values it then drops from the copy (synchronises s);
+// its values back in the reference order; y += A x and Y += A X over it.
+void build_chains(spc5cuda_mat* m, SortedPlan* plan, SpmvPart& part, cudaStream_t s);
+void unchain_values(const spc5cuda_mat* m, const SpmvPart& part, void* values, cudaStream_t s);
+void chain_part_spmv(const spc5cuda_mat* m, const SpmvPart& part, const void* x, void* y, bool mixed,
+                     cudaStream_t s);
+void chain_part_spmm(const spc5cuda_mat* m, const SpmvPart& part, int k, const void* x, long ldx, long xcs, void* y,
+                     long ldy, long ycs, bool mixed, cudaStream_t s);
+void launch_iota(long n, int* a, cudaStream_t s);
 // y += A x through the plan (x, y of the handle's types; mixed: F32 or
 // F32_V8 handle, float x, double y).  fork: run the parts concurrently on the
 // plan's two streams and join them back to s (one such call at a time per

@@ -7,12 +7,15 @@
 // accumulator sees the same FMA chain and y is bit-identical -- plus perm[i],
 // the block-row of y that sorted block-row i belongs to.  The sorted order is
 // cut into parts, each run by the kernel that suits its block-rows:
-//   * block-rows too large for the row kernel's chunks: cut into segments
-//     of at most L/32 of a chunk's buffers (greedy, in block order), the
-//     segments of 32 / L neighbouring block-rows interleaved so that a chunk
-//     holds segment k of each of them; the row kernel (L lanes per
-//     block-row) then stages them like short block-rows while every lane
-//     keeps its block-row's accumulators from chunk to chunk;
+//   * block-rows too large for the row kernel's chunks (above the class of
+//     L = 8 lanes), at r = 8: the chain part (chain.cu), one lane per
+//     (sub-row, column) multiply-add chain, chains sorted by length;
+//   * the same at r = 1, 2, 4: cut into segments of at most L/32 of a
+//     chunk's buffers (greedy, in block order), the segments of 32 / L
+//     neighbouring block-rows interleaved so that a chunk holds segment k of
+//     each of them; the row kernel (L lanes per block-row) then stages them
+//     like short block-rows while every lane keeps its block-row's
+//     accumulators from chunk to chunk;
 //   * the rest: the row kernel with L = 8, 4, 2 or 1 lanes per block-row,
 //     the smallest L whose chunk of 32 / L block-rows fits the staging
 //     buffers.  Block-rows of one chunk have about the same size, so no lane
@@ -49,11 +52,13 @@ __global__ void k_sorted_counts(int nbr, const int* __restrict__ perm, const int
     }
 }
 
-// The reference order back from the sorted copy, sorted block-rows
-// [a, nbr): sorted block-row i goes to block-row perm[i]'s offsets (one warp
-// per block-row).
+// The reference order back from the sorted copy: sorted block-row i goes to
+// block-row perm[i]'s offsets (one warp per block-row); headers of the
+// block-rows [a, nbr), values of [vfrom, nbr) (the others are in the chain
+// part or in segments).
 template <class V>
-__global__ void k_unsorted_copy(int a, int nbr, const int* __restrict__ perm, const int* __restrict__ sbrptr,
+__global__ void k_unsorted_copy(int a, int vfrom, int nbr, const int* __restrict__ perm,
+                                const int* __restrict__ sbrptr,
                                 const int* __restrict__ svalptr, const int* __restrict__ brptr,
                                 const int* __restrict__ valptr, int stride, const uint8_t* __restrict__ shdr,
                                 uint8_t* __restrict__ hdr, const V* __restrict__ svals, V* __restrict__ vals) {
@@ -64,6 +69,7 @@ __global__ void k_unsorted_copy(int a, int nbr, const int* __restrict__ perm, co
         const long h0 = long(sbrptr[i]) * stride, hn = long(sbrptr[i + 1]) * stride - h0;
         const long d0 = long(brptr[p]) * stride;
         for (long k = lane; k < hn; k += 32) hdr[d0 + k] = shdr[h0 + k];
+        if (i < vfrom) continue;
         const long v0 = svalptr[i], vn = long(svalptr[i + 1]) - v0;
         const long w0 = valptr[p];
         for (long k = lane; k < vn; k += 32) vals[w0 + k] = svals[v0 + k];
@@ -376,13 +382,14 @@ void build_sorted_plan(spc5cuda_mat* m, cudaStream_t s) {
     // boundary is at least the previous one (sizes descend)
     const int above8 = counts[0];
     int lo = above8;
-    if (above8 > 0) {
-        SpmvPart seg;
-        seg.lanes = seg_lanes(r);
-        seg.a = 0;
-        seg.b = above8;
-        seg.nseg = above8;
-        plan->parts.push_back(std::move(seg));
+    if (above8 > 0) {  // the chain part at r = 8, else the segmented part
+        SpmvPart big;
+        big.a = 0;
+        big.b = above8;
+        big.nseg = above8;
+        big.chains = r == 8;
+        big.lanes = big.chains ? 0 : seg_lanes(r);
+        plan->parts.push_back(std::move(big));
     }
     const int lanes_of[4] = {8, 4, 2, 1};
     for (int j = 0; j < 4; ++j) {
@@ -399,6 +406,10 @@ void build_sorted_plan(spc5cuda_mat* m, cudaStream_t s) {
     // ---- a balanced split of every part
     for (auto& part : plan->parts) {
         const int rows = part.b - part.a;
+        if (part.chains) {
+            build_chains(m, plan.get(), part, s);
+            continue;
+        }
         if (part.nseg > 0) {
             build_segments(m, plan.get(), part, stride, vbytes, s);
             continue;
@@ -432,35 +443,40 @@ void rebuild_original(const spc5cuda_mat* m, uint8_t* headers, void* values, cud
     const int stride = 4 + m->r * mask_bytes_of(m->value_type);
     const bool f64 = m->value_type == SPC5CUDA_F64;
     const int threads = 256;
-    const SpmvPart* seg = nullptr;
+    const SpmvPart* big = nullptr;
     for (const auto& part : p.parts)
-        if (part.nseg > 0) seg = &part;
-    const int nlong = seg ? seg->nseg : 0;
-    if (nbr > nlong) {
-        const int blocks = std::max(1, std::min(div_up(long(nbr - nlong) * 32, threads), sm_count() * 16));
+        if (part.nseg > 0) big = &part;
+    const int nlong = big ? big->nseg : 0;
+    // headers of the chain part are in plain sorted order, those of the
+    // segmented part in segment order (below)
+    const int a = big && !big->chains ? nlong : 0;
+    if (nbr > a) {
+        const int blocks = std::max(1, std::min(div_up(long(nbr - a) * 32, threads), sm_count() * 16));
         if (f64)
             k_unsorted_copy<double><<<blocks, threads, 0, s>>>(
-                nlong, nbr, p.perm.as<int>(), p.sbrptr.as<int>(), p.svalptr.as<int>(), m->brptr.as<int>(),
+                a, nlong, nbr, p.perm.as<int>(), p.sbrptr.as<int>(), p.svalptr.as<int>(), m->brptr.as<int>(),
                 m->valptr.as<int>(), stride, p.sheaders.as<uint8_t>(), headers, p.svalues.as<double>(),
                 static_cast<double*>(values));
         else
             k_unsorted_copy<float><<<blocks, threads, 0, s>>>(
-                nlong, nbr, p.perm.as<int>(), p.sbrptr.as<int>(), p.svalptr.as<int>(), m->brptr.as<int>(),
+                a, nlong, nbr, p.perm.as<int>(), p.sbrptr.as<int>(), p.svalptr.as<int>(), m->brptr.as<int>(),
                 m->valptr.as<int>(), stride, p.sheaders.as<uint8_t>(), headers, p.svalues.as<float>(),
                 static_cast<float*>(values));
         SPC5_CUDA(cudaGetLastError());
     }
-    if (nlong > 0) {
-        const int spw = 32 / seg->lanes;
+    if (big && big->chains) {
+        unchain_values(m, *big, values, s);
+    } else if (big) {
+        const int spw = 32 / big->lanes;
         const int blocks = std::max(1, std::min(div_up(long(nlong) * 32, threads), sm_count() * 16));
         if (f64)
             k_unsegmented_copy<double><<<blocks, threads, 0, s>>>(
-                nlong, spw, p.perm.as<int>(), seg->split.as<int>(), seg->vbrptr.as<int>(), seg->vvalptr.as<int>(),
+                nlong, spw, p.perm.as<int>(), big->split.as<int>(), big->vbrptr.as<int>(), big->vvalptr.as<int>(),
                 m->brptr.as<int>(), m->valptr.as<int>(), stride, p.sheaders.as<uint8_t>(), headers,
                 p.svalues.as<double>(), static_cast<double*>(values));
         else
             k_unsegmented_copy<float><<<blocks, threads, 0, s>>>(
-                nlong, spw, p.perm.as<int>(), seg->split.as<int>(), seg->vbrptr.as<int>(), seg->vvalptr.as<int>(),
+                nlong, spw, p.perm.as<int>(), big->split.as<int>(), big->vbrptr.as<int>(), big->vvalptr.as<int>(),
                 m->brptr.as<int>(), m->valptr.as<int>(), stride, p.sheaders.as<uint8_t>(), headers,
                 p.svalues.as<float>(), static_cast<float*>(values));
         SPC5_CUDA(cudaGetLastError());
@@ -497,7 +513,7 @@ BetaView plan_view(const spc5cuda_mat* m, const SpmvPart& part) {
 namespace {
 
 // Runs launch(view, stream) for every part of the plan: the parts write
-// disjoint rows of y, so the segmented part (the largest block-rows) runs on
+// disjoint rows of y, so the chain part (the largest block-rows) runs on
 // one plan stream, the smaller row-kernel parts on the other, the largest of
 // those on the caller's stream; all start after the work already queued on s
 // and s waits for all of them.
@@ -507,7 +523,7 @@ void run_parts(const spc5cuda_mat* m, cudaStream_t s, bool fork, F&& launch) {
     if (!fork) {
         // the parts one after another on the caller's stream: no shared plan
         // streams, so calls on different streams overlap freely
-        for (const auto& part : p.parts) launch(plan_view(m, part), s);
+        for (const auto& part : p.parts) launch(part, s);
         return;
     }
     std::lock_guard<std::mutex> lk(p.mu);
@@ -522,7 +538,7 @@ void run_parts(const spc5cuda_mat* m, cudaStream_t s, bool fork, F&& launch) {
     for (size_t i = 0; i < p.parts.size(); ++i) {
         const auto& part = p.parts[i];
         cudaStream_t st = (part.lanes == 0 || part.nseg) ? p.aux[0] : (int(i) == biggest ? s : p.aux[1]);
-        launch(plan_view(m, part), st);
+        launch(part, st);
     }
     for (int k = 0; k < 2; ++k) {
         SPC5_CUDA(cudaEventRecord(p.join[k], p.aux[k]));
@@ -534,7 +550,12 @@ void run_parts(const spc5cuda_mat* m, cudaStream_t s, bool fork, F&& launch) {
 
 void plan_spmv(const spc5cuda_mat* m, const void* x, void* y, bool mixed, cudaStream_t s, bool fork) {
     // the launchers pick the row kernel when the view has warp ranges
-    run_parts(m, s, fork, [&](const BetaView& v, cudaStream_t st) {
+    run_parts(m, s, fork, [&](const SpmvPart& part, cudaStream_t st) {
+        if (part.chains) {
+            chain_part_spmv(m, part, x, y, mixed, st);
+            return;
+        }
+        const BetaView v = plan_view(m, part);
         if (m->value_type == SPC5CUDA_F64)
             launch_spmv_f64(v, static_cast<const double*>(x), static_cast<double*>(y), st);
         else if (m->value_type == SPC5CUDA_F32_V8)
@@ -548,7 +569,12 @@ void plan_spmv(const spc5cuda_mat* m, const void* x, void* y, bool mixed, cudaSt
 
 void plan_spmm(const spc5cuda_mat* m, int k, const void* x, long ldx, long xcs, void* y, long ldy, long ycs,
                bool mixed, cudaStream_t s, bool fork) {
-    run_parts(m, s, fork, [&](const BetaView& v, cudaStream_t st) {
+    run_parts(m, s, fork, [&](const SpmvPart& part, cudaStream_t st) {
+        if (part.chains) {
+            chain_part_spmm(m, part, k, x, ldx, xcs, y, ldy, ycs, mixed, st);
+            return;
+        }
+        const BetaView v = plan_view(m, part);
         if (!v.wstart) throw Error(SPC5CUDA_ERR_INVALID, "plan part without warp ranges");
         if (m->value_type == SPC5CUDA_F64)
             launch_spmm_rows_f64(v, k, static_cast<const double*>(x), ldx, xcs, static_cast<double*>(y), ldy, ycs,

@@ -65,7 +65,8 @@ int plan_regime(const spc5cuda_mat* m, int r, const int* brptr, cudaStream_t s) 
 
 // A trial run: a temporary handle holding a copy of the CSR matrix is
 // converted to r the usual way (its default kernel choice: the row kernel or
-// the length-sorted plan) and its SpMV is timed (1 warm-up, 3 timed calls);
+// the length-sorted plan) and its SpMV is timed (2 warm-up calls, which also
+// load its kernels and size the library's scratch pool, then 5 timed calls);
 // returns microseconds per SpMV.
 double measure_us(const spc5cuda_mat* m, int r, cudaStream_t s) {
     spc5cuda_mat* t = nullptr;
@@ -91,15 +92,16 @@ double measure_us(const spc5cuda_mat* m, int r, cudaStream_t s) {
     SPC5_CUDA(cudaEventCreate(&e0));
     SPC5_CUDA(cudaEventCreate(&e1));
     run();
+    run();
     SPC5_CUDA(cudaEventRecord(e0, s));
-    for (int i = 0; i < 3; ++i) run();
+    for (int i = 0; i < 5; ++i) run();
     SPC5_CUDA(cudaEventRecord(e1, s));
     SPC5_CUDA(cudaEventSynchronize(e1));
     float ms = 0.f;
     SPC5_CUDA(cudaEventElapsedTime(&ms, e0, e1));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    return double(ms) * 1000.0 / 3.0;
+    return double(ms) * 1000.0 / 5.0;
 }
 
 }  // namespace

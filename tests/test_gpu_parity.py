@@ -264,10 +264,11 @@ def test_sorted_plan_in_place(cuda, vt, r):
         nbr = (csr.nrows + r - 1) // r
         vbytes = 8 if vt == S.F64 else 4
         # headers + values once, int32 offsets (brptr, valptr, perm, sorted
-        # offsets, partitions) and the segments' offsets (a few % of the
-        # beta arrays for a matrix of long rows cut into many segments)
+        # offsets, partitions), and for the values of the chain part (the
+        # largest block-rows) a 4-byte x index each plus, per chain, its
+        # length and id (at most 8 bytes per value), and slice padding
         beta = inf.header_bytes + csr.nnz * vbytes
-        assert inf.device_bytes <= 1.05 * beta + 7 * 4 * (nbr + 1) + (1 << 20), \
+        assert inf.device_bytes <= 1.05 * beta + 12 * csr.nnz + 7 * 4 * (nbr + 1) + (1 << 20), \
             (csr.name, inf.device_bytes, inf.header_bytes, csr.nnz)
         conv = oracle.csr_to_beta_v8 if mixed else oracle.csr_to_beta
         ob, oh, ov = conv(r, csr.rowptr, csr.colidx, csr.values.astype(dt))
