@@ -169,6 +169,7 @@ struct SpmvPart {
 struct SortedPlan {
     Owned sbrptr, sheaders, svalues, svalptr, perm;
     std::vector<SpmvPart> parts;
+    bool in_order = false;  // run the parts one after another on the caller's stream
     cudaStream_t aux[2] = {nullptr, nullptr};
     cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
     std::mutex mu;  // one fork/join at a time (the events are shared)

@@ -408,6 +408,12 @@ void build_sorted_plan(spc5cuda_mat* m, cudaStream_t s) {
         const int rows = part.b - part.a;
         if (part.chains) {
             build_chains(m, plan.get(), part, s);
+            // FP64: the chain part and the row kernel's part contend for the
+            // SMs' load pipes; one after the other they take 563 against 688
+            // us concurrently (power-law N = 4M, r = 8, B200).  The float
+            // layouts gain a little from running them concurrently (662
+            // against 678 us).
+            plan->in_order = m->value_type == SPC5CUDA_F64;
             continue;
         }
         if (part.nseg > 0) {
@@ -512,15 +518,16 @@ BetaView plan_view(const spc5cuda_mat* m, const SpmvPart& part) {
 
 namespace {
 
-// Runs launch(view, stream) for every part of the plan: the parts write
-// disjoint rows of y, so the chain part (the largest block-rows) runs on
-// one plan stream, the smaller row-kernel parts on the other, the largest of
-// those on the caller's stream; all start after the work already queued on s
-// and s waits for all of them.
+// Runs launch(part, stream) for every part of the plan: the parts write
+// disjoint rows of y, so the part of the largest block-rows runs on one plan
+// stream, the smaller row-kernel parts on the other, the largest of those on
+// the caller's stream; all start after the work already queued on s and s
+// waits for all of them.  Without fork, or for a plan whose parts run
+// faster in order (in_order), they run one after another on s.
 template <class F>
 void run_parts(const spc5cuda_mat* m, cudaStream_t s, bool fork, F&& launch) {
     SortedPlan& p = *m->plan;
-    if (!fork) {
+    if (!fork || p.in_order) {
         // the parts one after another on the caller's stream: no shared plan
         // streams, so calls on different streams overlap freely
         for (const auto& part : p.parts) launch(part, s);
