@@ -8,9 +8,9 @@
 // the block-row of y that sorted block-row i belongs to.  The sorted order is
 // cut into parts, each run by the kernel that suits its block-rows:
 //   * block-rows too large for the row kernel's chunks (above the class of
-//     L = 8 lanes), at r = 8: the chain part (chain.cu), one lane per
+//     L = 8 lanes), at r = 2, 4, 8: the chain part (chain.cu), one lane per
 //     (sub-row, column) multiply-add chain, chains sorted by length;
-//   * the same at r = 1, 2, 4: cut into segments of at most L/32 of a
+//   * the same at r = 1: cut into segments of at most L/32 of a
 //     chunk's buffers (greedy, in block order), the segments of 32 / L
 //     neighbouring block-rows interleaved so that a chunk holds segment k of
 //     each of them; the row kernel (L lanes per block-row) then stages them
@@ -382,12 +382,17 @@ void build_sorted_plan(spc5cuda_mat* m, cudaStream_t s) {
     // boundary is at least the previous one (sizes descend)
     const int above8 = counts[0];
     int lo = above8;
-    if (above8 > 0) {  // the chain part at r = 8, else the segmented part
+    if (above8 > 0) {
+        // the chain part for r >= 2, the segmented part at r = 1, measured
+        // on B200 (power-law N = 4M, FP64 / mixed us per SpMV): chains at
+        // r = 2 497 / 519 against segments 568 / 608, r = 4 519 / 560
+        // against 651 / 785, r = 8 564 / 761 against 940 / 784; segments at
+        // r = 1 475 / 369 against chains 527 / 576
         SpmvPart big;
         big.a = 0;
         big.b = above8;
         big.nseg = above8;
-        big.chains = r == 8;
+        big.chains = r >= 2;
         big.lanes = big.chains ? 0 : seg_lanes(r);
         plan->parts.push_back(std::move(big));
     }
