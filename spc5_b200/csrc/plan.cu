@@ -413,12 +413,11 @@ void build_sorted_plan(spc5cuda_mat* m, cudaStream_t s) {
         const int rows = part.b - part.a;
         if (part.chains) {
             build_chains(m, plan.get(), part, s);
-            // FP64: the chain part and the row kernel's part contend for the
-            // SMs' load pipes; one after the other they take 563 against 688
-            // us concurrently (power-law N = 4M, r = 8, B200).  The float
-            // layouts gain a little from running them concurrently (662
-            // against 678 us).
-            plan->in_order = m->value_type == SPC5CUDA_F64;
+            // the chain part and the row kernel's parts contend for the
+            // SMs' load pipes: one after the other they run faster than
+            // concurrently (power-law N = 4M, r = 8, B200: FP64 563 against
+            // 688 us, mixed 8-column layout 679 against 759 us)
+            plan->in_order = true;
             continue;
         }
         if (part.nseg > 0) {
