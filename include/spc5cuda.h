@@ -193,15 +193,21 @@ SPC5CUDA_API spc5cuda_status spc5cuda_mat_info(const spc5cuda_mat* mat, spc5cuda
  *             stream);
  *   ROWS   -- the thread-per-sub-row kernel; SPC5CUDA_ERR_UNSUPPORTED on a
  *             converted matrix with a block-row that does not fit;
- *   SORTED -- the length-sorted plan: the handle keeps a second copy of the
- *             matrix with its block-rows sorted by size, and SpMV runs each
- *             size class with the kernel and lanes per block-row that suit
- *             it.  AUTO uses it when some block-row does not fit the row
- *             kernel (power-law and other irregular matrices).
+ *   SORTED -- the length-sorted plan: the handle holds its headers and
+ *             values with the block-rows sorted by size (the largest ones
+ *             as multiply-add chains at r = 2, 4, 8, in segments at r = 1)
+ *             instead of in the reference order, and SpMV runs each size
+ *             class with the kernel and lanes per block-row that suit it.
+ *             AUTO uses it when some block-row does not fit the row kernel
+ *             (power-law and other irregular matrices).
  * spc5cuda_mat_kernel reports the kernel SpMV uses now (GROUPS, ROWS or
  * SORTED; AUTO before conversion).  Selecting SORTED (or AUTO, where it picks
- * the plan) on a converted matrix builds the sorted copy; selecting GROUPS or
- * ROWS releases it.  Both synchronise the device. */
+ * the plan) on a converted matrix builds the plan and releases the
+ * reference-order arrays; selecting GROUPS or ROWS rebuilds them from the
+ * plan and releases the plan.  Both synchronise the device.
+ * spc5cuda_get_arrays and spc5cuda_decode_coo return the reference order
+ * whichever form the handle holds; spc5cuda_batch_create rebuilds it into the
+ * handle (which then holds both). */
 #define SPC5CUDA_KERNEL_AUTO 0
 #define SPC5CUDA_KERNEL_GROUPS 1
 #define SPC5CUDA_KERNEL_ROWS 2
