@@ -925,7 +925,7 @@ def run_serve(args):
 # so roofline.traffic of the full workloads is these ratios times their bytes.
 L2_BYTES = 126e6  # B200 L2
 
-TRAFFIC_RATIO = {"powerlaw": {1: 1.200, 2: 1.224, 4: 1.156, 8: 1.198},
+TRAFFIC_RATIO = {"powerlaw": {1: 1.199, 2: 1.203, 4: 1.168, 8: 1.593},
                  "stencil27": {1: 0.999, 2: 0.984, 4: 0.978, 8: 0.994}}
 
 # spc5cuda_mat_kernel codes: SPC5CUDA_KERNEL_GROUPS = 1, SPC5CUDA_KERNEL_ROWS = 2

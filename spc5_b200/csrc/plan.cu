@@ -380,18 +380,24 @@ void build_sorted_plan(spc5cuda_mat* m, cudaStream_t s) {
     }
     // counts[j]: block-rows above the limit of L = 8 >> j lanes; every
     // boundary is at least the previous one (sizes descend)
-    const int above8 = counts[0];
-    int lo = above8;
-    if (above8 > 0) {
-        // the chain part for r >= 2, the segmented part at r = 1, measured
-        // on B200 (power-law N = 4M, FP64 / mixed us per SpMV): chains at
-        // r = 2 497 / 519 against segments 568 / 608, r = 4 519 / 560
-        // against 651 / 785, r = 8 564 / 761 against 940 / 784; segments at
-        // r = 1 475 / 369 against chains 527 / 576
+    // the chain part for r >= 2, the segmented part at r = 1, measured on B200
+    // (power-law N = 4M, FP64 / mixed us per SpMV): chains at r = 2 497 / 519
+    // against segments 568 / 608, r = 4 519 / 560 against 651 / 785, r = 8
+    // 564 / 761 against 940 / 784; segments at r = 1 475 / 369 against chains
+    // 527 / 576.  The chain part takes the block-rows above the limit of
+    // 8 >> chain_class[r] lanes (the smaller ones run faster as chains than on
+    // the row kernel too): r = 2 above 2 lanes (408 / 405 us, against 501 /
+    // 518 above 8 and 548 / 508 with every block-row in chains), r = 4 above 4
+    // lanes (459 / 487 against 517 / 575), r = 8 above 2 lanes (548 / 509
+    // against 563 / 679)
+    static constexpr int chain_class[9] = {0, 0, 2, 0, 1, 0, 0, 0, 2};
+    const int nbig = r >= 2 ? counts[chain_class[r]] : counts[0];
+    int lo = nbig;
+    if (nbig > 0) {
         SpmvPart big;
         big.a = 0;
-        big.b = above8;
-        big.nseg = above8;
+        big.b = nbig;
+        big.nseg = nbig;
         big.chains = r >= 2;
         big.lanes = big.chains ? 0 : seg_lanes(r);
         plan->parts.push_back(std::move(big));
