@@ -135,8 +135,9 @@ SPC5CUDA_API spc5cuda_status spc5cuda_core_spmv_f32(int r, long nbRows, const in
  * device array of ~4.5 MB that every GPU loading the library keeps until the
  * process exits.  Limit: ceil(nbRows / r) <= 1,048,576 block-rows, else
  * SPC5CUDA_ERR_INVALID.  The first call on a device looks up the array's
- * address with that device current, so make it before any stream capture.
- * All calls share the array: calls that overlap on the GPU (other streams or
+ * address with that device current, so make it before any stream capture;
+ * the address is kept for the process, so do not call this entry point on a
+ * device after cudaDeviceReset of that device.  All calls share the array: calls that overlap on the GPU (other streams or
  * threads without ordering) race; order them on one stream. */
 SPC5CUDA_API spc5cuda_status spc5cuda_core_spmv_f64_noalloc(int r, long nbRows,
                                                             const int* rowsSizes,
