@@ -20,24 +20,27 @@ namespace {
 // the time per value keyed by the average number of values per block, as the
 // reference's SPC5_find_best model is (src/spc5.hpp:1157-1212).
 // Value type (F64, F32, F32_V8) x r (1, 2, 4, 8) x regime: {t0, d0, d1, d2}.
+// The sorted-plan rows were refitted after the plan's chain part (r = 2, 4,
+// 8) on the plan-regime calibration matrices alone (power-law and random,
+// tune_fit.plan_calibration_set), keeping the row-kernel t0.
 constexpr double kModel[3][4][2][4] = {
     {
-        {{1.027079e+01, -2.714134e-07, 9.285081e-06, 1.994012e-06}, {1.027079e+01, 1.134102e-05, 0.000000e+00, 0.000000e+00}},
-        {{1.046586e+01, 6.170896e-07, 9.230068e-06, 9.138698e-06}, {1.046586e+01, 1.525453e-05, 0.000000e+00, 0.000000e+00}},
-        {{1.004610e+01, 1.547721e-06, 1.189384e-05, 2.402879e-05}, {1.004610e+01, 1.887387e-05, 0.000000e+00, 0.000000e+00}},
-        {{1.004540e+01, 6.250567e-07, 5.782892e-05, -8.901463e-05}, {1.004540e+01, 3.599312e-05, 0.000000e+00, 0.000000e+00}},
+        {{1.027079e+01, -2.714134e-07, 9.285081e-06, 1.994012e-06}, {1.027079e+01, 1.113738e-05, 0.000000e+00, 0.000000e+00}},
+        {{1.046586e+01, 6.170896e-07, 9.230068e-06, 9.138698e-06}, {1.046586e+01, 1.212031e-05, 0.000000e+00, 0.000000e+00}},
+        {{1.004610e+01, 1.547721e-06, 1.189384e-05, 2.402879e-05}, {1.004610e+01, 8.274836e-06, 0.000000e+00, 0.000000e+00}},
+        {{1.004540e+01, 6.250567e-07, 5.782892e-05, -8.901463e-05}, {1.004540e+01, 7.059285e-06, 0.000000e+00, 0.000000e+00}},
     },
     {
-        {{1.009044e+01, 2.953275e-07, 6.279096e-06, 1.099184e-05}, {1.009044e+01, 9.677628e-06, 0.000000e+00, 0.000000e+00}},
-        {{1.008880e+01, 1.137428e-06, 1.740009e-06, 3.621405e-05}, {1.008880e+01, 1.482245e-05, 0.000000e+00, 0.000000e+00}},
-        {{1.020511e+01, 1.170424e-06, 1.023505e-05, 1.026359e-04}, {1.020511e+01, 3.810895e-05, 0.000000e+00, 0.000000e+00}},
-        {{1.034971e+01, -4.723864e-07, 8.071517e-05, -1.176461e-04}, {1.034971e+01, 4.555848e-05, 0.000000e+00, 0.000000e+00}},
+        {{1.009044e+01, 2.953275e-07, 6.279096e-06, 1.099184e-05}, {1.009044e+01, 9.763137e-06, 0.000000e+00, 0.000000e+00}},
+        {{1.008880e+01, 1.137428e-06, 1.740009e-06, 3.621405e-05}, {1.008880e+01, 1.172209e-05, 0.000000e+00, 0.000000e+00}},
+        {{1.020511e+01, 1.170424e-06, 1.023505e-05, 1.026359e-04}, {1.020511e+01, 6.684552e-06, 0.000000e+00, 0.000000e+00}},
+        {{1.034971e+01, -4.723864e-07, 8.071517e-05, -1.176461e-04}, {1.034971e+01, 5.902880e-06, 0.000000e+00, 0.000000e+00}},
     },
     {
-        {{9.690487e+00, -8.483423e-07, 1.129287e-05, 5.480109e-06}, {9.690487e+00, 1.022678e-05, 0.000000e+00, 0.000000e+00}},
-        {{9.904177e+00, 1.562250e-07, 1.131417e-05, 1.759617e-05}, {9.904177e+00, 1.857101e-05, 0.000000e+00, 0.000000e+00}},
-        {{1.008765e+01, 1.592180e-07, 2.480687e-05, 2.707475e-05}, {1.008765e+01, 2.423231e-05, 0.000000e+00, 0.000000e+00}},
-        {{1.044845e+01, -1.152926e-06, 8.811726e-05, -7.893453e-05}, {1.044845e+01, 4.799635e-05, 0.000000e+00, 0.000000e+00}},
+        {{9.690487e+00, -8.483423e-07, 1.129287e-05, 5.480109e-06}, {9.690487e+00, 1.023616e-05, 0.000000e+00, 0.000000e+00}},
+        {{9.904177e+00, 1.562250e-07, 1.131417e-05, 1.759617e-05}, {9.904177e+00, 1.203661e-05, 0.000000e+00, 0.000000e+00}},
+        {{1.008765e+01, 1.592180e-07, 2.480687e-05, 2.707475e-05}, {1.008765e+01, 7.725355e-06, 0.000000e+00, 0.000000e+00}},
+        {{1.044845e+01, -1.152926e-06, 8.811726e-05, -7.893453e-05}, {1.044845e+01, 6.381369e-06, 0.000000e+00, 0.000000e+00}},
     },
 };
 

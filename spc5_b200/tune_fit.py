@@ -17,6 +17,8 @@ measured on a B200 with this project's kernels, for r = 1, 2, 4 and 8.
 
     python -m spc5_b200.tune_fit measure > calib.jsonl   # on a B200
     python -m spc5_b200.tune_fit fit calib.jsonl          # prints the C table
+    python -m spc5_b200.tune_fit measure_plan > plan.jsonl           # plan regime only
+    python -m spc5_b200.tune_fit refit_plan plan.jsonl spc5_b200/csrc/tune.cu
 
 ``fit`` prints the table pasted into csrc/tune.cu (kModel) and the fraction of
 calibration matrices whose modelled pick is within 10% of the best measured r
@@ -52,8 +54,14 @@ def calibration_set():
         out.append(M.banded(50_000, bw, d, seed=bw))
     out += [M.stencil27(g) for g in (30, 60, 100)]
     out += [M.poisson2d(g) for g in (128, 256, 512)]
-    out += [M.powerlaw(n, seed=40 + k) for k, n in enumerate((100_000, 200_000, 300_000, 500_000, 1_000_000,
-                                                              2_000_000))]
+    return out + plan_calibration_set()
+
+
+def plan_calibration_set():
+    """The matrices of the calibration set whose block-rows do not all fit
+    the row kernel (the sorted-plan regime): power-law and random."""
+    out = [M.powerlaw(n, seed=40 + k) for k, n in enumerate((100_000, 200_000, 300_000, 500_000, 1_000_000,
+                                                             2_000_000))]
     for n, per_row, seed in ((200_000, 20, 5), (100_000, 50, 6)):
         g = np.random.default_rng(seed)
         rows = np.repeat(np.arange(n), per_row)
@@ -63,12 +71,12 @@ def calibration_set():
     return out
 
 
-def measure(reps: int = 10, warmup: int = 3) -> None:
+def measure(reps: int = 10, warmup: int = 3, mats=None) -> None:
     import torch
 
     import spc5_b200 as S
     torch.cuda.set_device(0)
-    for idx, csr in enumerate(calibration_set()):
+    for idx, csr in enumerate(calibration_set() if mats is None else mats):
         for vt in (S.F64, S.F32, S.F32_V8):
             for r in RS:
                 dt = np.float64 if vt == S.F64 else np.float32
@@ -102,6 +110,28 @@ def _feats(p):
 def _regime(p):
     """0: row kernel, 1: length-sorted plan (recorded by ``measure``)."""
     return int(p["plan"])
+
+
+def refit_plan(path: str, table: str) -> None:
+    """Refits the sorted-plan rows of the table in ``table`` (a tune.cu) from
+    the timings in ``path`` (``measure_plan``), keeping each row's t0: one
+    cost per value per value type and r, as ``fit`` does."""
+    import re
+    src = open(table).read()
+    start = src.index("constexpr double kModel")
+    body = src[start:src.index("};", start)]
+    K = np.array([float(x) for x in re.findall(r"-?\d\.\d+e[+-]\d+", body)]).reshape(3, 4, 2, 4)
+    rows = [json.loads(l) for l in open(path) if l.strip()]
+    for vt in (0, 1, 2):
+        for ri, r in enumerate(RS):
+            pts = [p for p in rows if p["vt"] == vt and p["r"] == r and p["plan"] == 1]
+            if not pts:
+                continue
+            t0 = K[vt, ri, 0, 0]
+            nnz = np.array([float(p["nnz"]) for p in pts])
+            us = np.array([p["us"] for p in pts])
+            d0 = float(np.sum((us - t0) / us * nnz / us) / np.sum((nnz / us) ** 2))
+            print(f"// value type {vt}, r = {r}: sorted-plan {{t0, d0}} = {{{t0:.6e}, {d0:.6e}}}")
 
 
 def fit(path: str) -> None:
@@ -156,6 +186,10 @@ def fit(path: str) -> None:
 if __name__ == "__main__":
     if len(sys.argv) >= 2 and sys.argv[1] == "measure":
         measure()
+    elif len(sys.argv) >= 2 and sys.argv[1] == "measure_plan":
+        measure(mats=plan_calibration_set())
+    elif len(sys.argv) >= 4 and sys.argv[1] == "refit_plan":
+        refit_plan(sys.argv[2], sys.argv[3])
     elif len(sys.argv) >= 3 and sys.argv[1] == "fit":
         fit(sys.argv[2])
     else:
