@@ -68,6 +68,8 @@ def lib():
         l.oracle_block_count.argtypes = [_I, _I, _I, _P, _P]
         l.oracle_blockrow_counts.restype = None
         l.oracle_blockrow_counts.argtypes = [_I, _I, _I, _P, _P, _P]
+        l.oracle_beta_spmv_f64_chains.restype = _I
+        l.oracle_beta_spmv_f64_chains.argtypes = [_I, _I, _P, _P, _P, _P, _P]
         for name in ("oracle_beta_spmv_f64", "oracle_beta_spmv_f32", "oracle_beta_spmv_mixed"):
             f = getattr(l, name)
             f.restype = None
@@ -146,6 +148,19 @@ def beta_spmv_f64(r, nrows, brptr, headers, values, x, y):
     assert y.dtype == np.float64 and y.flags.c_contiguous
     lib().oracle_beta_spmv_f64(r, nrows, _ptr(_i32(brptr)), _ptr(np.ascontiguousarray(headers)),
                                _ptr(np.ascontiguousarray(values, dtype=np.float64)), _ptr(xp), _ptr(y))
+    return y
+
+
+def beta_spmv_f64_chains(r, nrows, brptr, headers, values, x, y):
+    """y += A x evaluated as per-(sub-row, column) multiply-add chains (the
+    CUDA chain part's form); equals beta_spmv_f64 bit for bit for finite x."""
+    xp = x_padded(np.ascontiguousarray(x, dtype=np.float64))
+    assert y.dtype == np.float64 and y.flags.c_contiguous
+    st = lib().oracle_beta_spmv_f64_chains(r, nrows, _ptr(_i32(brptr)), _ptr(np.ascontiguousarray(headers)),
+                                           _ptr(np.ascontiguousarray(values, dtype=np.float64)), _ptr(xp),
+                                           _ptr(y))
+    if st != 0:
+        raise MemoryError("oracle_beta_spmv_f64_chains")
     return y
 
 

@@ -32,6 +32,7 @@
  */
 #include <math.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 #include <limits.h>
 
@@ -305,6 +306,71 @@ void oracle_beta_spmv_mixed(int r, int nrows, const int* brptr, const uint8_t* h
         }
         for (int i = 0; i < r && row0 + i < nrows; ++i) y[row0 + i] += tree16d(acc[i]);
     }
+}
+
+/*
+ * The same FP64 product regrouped as multiply-add chains, the form in which
+ * the CUDA path runs the largest block-rows of irregular matrices: the
+ * accumulator of (sub-row i, column c) in oracle_beta_spmv_f64 above
+ * (spc5.hpp:2309-2632) only changes at the blocks whose mask i has bit c,
+ * so its chain is the list of those values and x indices in block order;
+ * each chain is evaluated from +0.0 on its own, then the reduce_add tree of
+ * the 8 chain results of a sub-row is added to y.  The reference's
+ * fma(0, x, acc) at a clear bit leaves acc unchanged for finite x (acc starts
+ * at +0.0 and never becomes -0.0 in round-to-nearest), so for finite x this
+ * equals oracle_beta_spmv_f64 bit for bit.  Returns 0, or -1 when out of
+ * memory.
+ */
+int oracle_beta_spmv_f64_chains(int r, int nrows, const int* brptr, const uint8_t* headers,
+                                const double* values, const double* x, double* y) {
+    const int stride = 4 + r;
+    const int nbr = (nrows + r - 1) / r;
+    long cap = 0;
+    for (int br = 0; br < nbr; ++br) {
+        const long nb = brptr[br + 1] - brptr[br];
+        if (nb > cap) cap = nb;
+    }
+    /* chain (i, c) of a block-row holds at most one entry per block */
+    double* cval = (double*)malloc(sizeof(double) * (size_t)(64 * (cap > 0 ? cap : 1)));
+    int* ccol = (int*)malloc(sizeof(int) * (size_t)(64 * (cap > 0 ? cap : 1)));
+    if (!cval || !ccol) {
+        free(cval);
+        free(ccol);
+        return -1;
+    }
+    const double* v = values;
+    for (int br = 0; br < nbr; ++br) {
+        int len[8][8];
+        memset(len, 0, sizeof(len));
+        for (int b = brptr[br]; b < brptr[br + 1]; ++b) {
+            const uint8_t* h = headers + (long)b * stride;
+            const int col = rd_i32(h);
+            for (int i = 0; i < r; ++i) {
+                const unsigned m = h[4 + i];
+                for (int c = 0; c < 8; ++c) {
+                    if ((m >> c) & 1u) {
+                        const long e = (long)(i * 8 + c) * cap + len[i][c]++;
+                        cval[e] = *v++;
+                        ccol[e] = col + c;
+                    }
+                }
+            }
+        }
+        const int row0 = br * r;
+        for (int i = 0; i < r && row0 + i < nrows; ++i) {
+            double a[8];
+            for (int c = 0; c < 8; ++c) {
+                double acc = 0.0;
+                const long e0 = (long)(i * 8 + c) * cap;
+                for (int j = 0; j < len[i][c]; ++j) acc = fma(cval[e0 + j], x[ccol[e0 + j]], acc);
+                a[c] = acc;
+            }
+            y[row0 + i] += ((a[0] + a[4]) + (a[2] + a[6])) + ((a[1] + a[5]) + (a[3] + a[7]));
+        }
+    }
+    free(cval);
+    free(ccol);
+    return 0;
 }
 
 /*
