@@ -14,8 +14,9 @@
 // lanes often run neighbouring columns of one sub-row and share x lines) and
 // cut into slices of 32 (one warp each, the longest first); entry j of the
 // slice's lane l is at slice_off[slice] + 32 j + l, so a warp's value and
-// index loads are coalesced and its lanes finish together.  Empty chains are not stored: a
-// bit mask per sub-row marks its non-empty ones.  A second launch adds each
+// index loads are coalesced and its lanes finish together.  Empty chains are
+// not stored: a bit mask per sub-row marks its non-empty ones.  A second
+// launch adds each
 // sub-row's VS chain results (+0 for the empty ones, the reference's
 // untouched accumulators) with the reduce tree into y.  Every chain runs
 // the reference's multiply-adds in the reference's order: y is
@@ -39,7 +40,9 @@ constexpr unsigned FULL = 0xFFFFFFFFu;
 // than 16 entries on average: the part of a large r) it is compiled for 4
 // resident CTAs per SM, so that more chains are in flight; long chains (small
 // r) keep the registers for the next step's loads.  Measured on B200,
-// power-law N = 4M: r = 8 645 against 669 us, r = 1 540 against 576 us.
+// power-law N = 4M, with the chain part for the block-rows above 8 lanes
+// (r = 1 then ran chains too): r = 8 645 against 669 us, r = 1 540 against
+// 576 us.
 constexpr int CHAIN_U = 8;
 constexpr int CHAIN_SHORT = 16;
 
