@@ -11,16 +11,15 @@
 // and one lane runs one chain with no header decode and no empty column
 // slots.  The chains are sorted by length class (lengths within about 1/8 of
 // one another; chains of one class stay in chain-id order, so neighbouring
-// lanes often run neighbouring columns of one sub-row and share x lines) and
+// lanes often run neighbouring columns of one sub-row) and
 // cut into slices of 32 (one warp each, the longest first); entry j of the
 // slice's lane l is at slice_off[slice] + 32 j + l, so a warp's value and
 // index loads are coalesced and its lanes finish together.  Empty chains are
 // not stored: a bit mask per sub-row marks its non-empty ones.  A second
-// launch adds each
-// sub-row's VS chain results (+0 for the empty ones, the reference's
-// untouched accumulators) with the reduce tree into y.  Every chain runs
-// the reference's multiply-adds in the reference's order: y is
-// bit-identical.
+// launch adds each sub-row's VS chain results (+0 for the empty ones, the
+// reference's untouched accumulators) with the reduce tree into y.  Every
+// chain runs the reference's multiply-adds in the reference's order: y is
+// bit-identical for finite x.
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
